@@ -1,0 +1,381 @@
+"""Benchmark: plain DeepWalk on a dynamic R-MAT graph (scale 20, ~16M edges,
+log-uniform weights in [1, 2^20)). One step = one update batch of 100K edges
+(50K absent-pair inserts + 50K uniform deletes) followed by 1M DeepWalk walks
+of length 80 (one per vertex), one launch per job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` = walk steps per second over the whole
+device-timed step (updates included), inputs resident in HBM; `e2e` = the same
+metric through the C ABI with pinned host buffers (batches copied in, every
+walk row copied out, inside the timed region). With N > 1 (torchrun) every
+rank runs a full replica (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EDGE_FACTOR = 20, 16
+W_LO, W_HI = 1, 1 << 20
+WALK_LEN = 80
+BATCH_INS, BATCH_DEL = 50_000, 50_000
+GRAPH_SEED = 1234 + 2
+BYTES_PER_STEP = 32  # algorithmic bytes per produced walk step (vertex 8, alias 8, member 4+4, group 4, store 4)
+WORKLOAD = "plain-deepwalk-rmat20"
+
+
+def make_workload(steps_total: int):
+    from bingo_b200 import gen
+    n = 1 << SCALE
+    src, dst = gen.rmat(SCALE, EDGE_FACTOR, seed=GRAPH_SEED)
+    w = gen.weights(len(src), gen.W_LOGUNIFORM, W_LO, W_HI, seed=GRAPH_SEED + 1)
+    ug = gen.UpdateGen(n, src, dst, seed=GRAPH_SEED + 2)
+    batches = []
+    for _ in range(steps_total):
+        ins = ug.inserts(BATCH_INS, gen.W_LOGUNIFORM, W_LO, W_HI)
+        dels = ug.deletes(BATCH_DEL)
+        batches.append((ins, dels))
+    return n, src, dst, w, batches
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_step():
+    """DRAM bytes per produced step of the walk kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "walk_deepwalk_rmat20.md")
+    try:
+        m = re.search(r"dram_bytes_per_step:\s*([0-9.]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bingo_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------- CPU leg
+def cpu_sample(n, src, dst, w, batch, walks: int, seed: int):
+    """Time the oracle (OpenMP, all host threads) on one full update batch and
+    `walks` DeepWalk walks; extrapolate to a full step (n walks)."""
+    from oracle import pyoracle as po
+    ex = po.ExactGraph(n)
+    ex.load(src, dst, w)
+    (ins, dels) = batch
+    t0 = time.perf_counter()
+    ex.insert(*ins)
+    ex.delete(*dels)
+    t_upd = time.perf_counter() - t0
+    rng = np.random.default_rng(seed)
+    starts = np.sort(rng.choice(n, size=walks, replace=False)).astype(np.uint32)
+    t0 = time.perf_counter()
+    rows = ex.walk(0, WALK_LEN, starts, seed=seed, job_id=0)
+    t_walk = time.perf_counter() - t0
+    steps = int((rows >= 0).sum() - len(starts))
+    scale = n / walks
+    value = steps * scale / (t_upd + t_walk * scale)
+    return dict(value=value, t_update=t_upd, t_walk=t_walk, walk_steps=steps, walks=walks,
+                walk_steps_per_s=steps / t_walk, edge_updates_per_s=(len(ins[0]) + len(dels[0])) / t_upd)
+
+
+def run_reference(args):
+    """The reference arm: the reference has no CPU implementation of the path,
+    so the CPU oracle port (OpenMP, all host threads) stands in for it, on the
+    same graph and batches; each step is one full update batch plus a bounded
+    walk sample, extrapolated to the full step."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    n, src, dst, w, batches = make_workload(args.warmup + args.steps)
+    walks = args.ref_walks
+    vals, last = [], None
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(n, src, dst, w, batches[i], walks, seed=100 + i)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            last = r
+    value = float(np.mean(vals))
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": "walk_steps_per_s", "value": value, "unit": "steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "weights": "loguniform[1,2^20)",
+                   "walks": n, "walk_len": WALK_LEN, "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"per step: one full 50K+50K update batch + {walks} walks x {WALK_LEN}, "
+                                   f"walk time scaled to {n} walks"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "walk_steps_per_s": last["walk_steps_per_s"], "edge_updates_per_s": last["edge_updates_per_s"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    from bingo_b200 import DEEPWALK, PLAIN, Graph, WalkJob
+
+    total = args.warmup + args.steps
+    n, src, dst, w, batches = make_workload(total)
+    stream = torch.cuda.current_stream(dev)
+    g = Graph(device=local, synchronous=False)
+    g.set_stream(stream.cuda_stream)
+    g.load_edges(src, dst, w, n)
+    g.sync()
+
+    def dev_i32(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)
+
+    dbatches = [((dev_i32(i[0]), dev_i32(i[1]), dev_i32(i[2])), (dev_i32(d[0]), dev_i32(d[1]))) for i, d in batches]
+    out = torch.empty((n, WALK_LEN), dtype=torch.int32, device=dev)
+    slots = torch.empty(BATCH_INS, dtype=torch.int32, device=dev)
+    seed = 0xB1460 + rank
+
+    ev = {k: [torch.cuda.Event(enable_timing=True) for _ in range(total)] for k in ("u0", "u1", "w1")}
+
+    def step(i):
+        (a, b, c), (du, ds) = dbatches[i]
+        ev["u0"][i].record(stream)
+        g.insert_batch(a, b, c, out_slots=slots)
+        g.delete_batch(du, ds)
+        ev["u1"][i].record(stream)
+        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, starts=None, n_starts=n, first=0, job_id=i, seed=seed,
+                             out=out)], mode=PLAIN)
+        ev["w1"][i].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+    g.sync()
+    torch.cuda.synchronize(dev)
+    st0 = g.stats()
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.warmup, total):
+        step(i)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    g.sync()
+    st1 = g.stats()
+    ms = t_start.elapsed_time(t_end)
+    walk_ms = sum(ev["u1"][i].elapsed_time(ev["w1"][i]) for i in range(args.warmup, total))
+    upd_ms = sum(ev["u0"][i].elapsed_time(ev["u1"][i]) for i in range(args.warmup, total))
+    steps_local = st1["walk_steps"] - st0["walk_steps"]
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    ms_max = reduce_max(ms, world, dev)
+    steps_all = reduce_sum(steps_local, world, dev)
+    value = steps_all / (ms_max / 1e3)
+
+    # ---- e2e: same work through the C ABI with pinned host buffers
+    g.load_edges(src, dst, w, n)
+    g.sync()
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory()
+        return t
+
+    hbatches = [((pinned(i[0]), pinned(i[1]), pinned(i[2])), (pinned(d[0]), pinned(d[1]))) for i, d in batches]
+    hout = torch.empty((n, WALK_LEN), dtype=torch.int32).pin_memory()
+    hslots = torch.empty(BATCH_INS, dtype=torch.int32).pin_memory()
+
+    def e2e_step(i):
+        (a, b, c), (du, ds) = hbatches[i]
+        g.insert_batch(a, b, c, out_slots=hslots)
+        g.delete_batch(du, ds)
+        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, starts=None, n_starts=n, first=0, job_id=i, seed=seed,
+                             out=hout)], mode=PLAIN)
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    g.sync()
+    torch.cuda.synchronize(dev)
+    st2 = g.stats()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.warmup, total):
+        e2e_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    g.sync()
+    st3 = g.stats()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), world, dev)
+    e2e_steps = reduce_sum(st3["walk_steps"] - st2["walk_steps"], world, dev)
+    h2d = BATCH_INS * 12 + BATCH_DEL * 8
+    d2h = n * WALK_LEN * 4 + BATCH_INS * 4
+
+    # ---- roofline of the walk kernel
+    peak, peak_src = peak_hbm()
+    achieved = steps_local * BYTES_PER_STEP / (walk_ms / 1e3) / 1e9
+    tps = traffic_per_step()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": (tps * steps_local / args.steps) if tps else None, "peak_source": peak_src,
+            "kernel": "k_walk_plain<DEEPWALK>", "bytes_per_step": BYTES_PER_STEP}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_sample(n, src, dst, w, batches[args.warmup], args.cpu_walks, seed=7)
+        cpu = {"value": r["value"], "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"one full 50K+50K update batch + {args.cpu_walks} walks x {WALK_LEN} on the CPU oracle "
+                         f"(OpenMP), walk time scaled to {n} walks",
+               "walk_steps_per_s": r["walk_steps_per_s"], "edge_updates_per_s": r["edge_updates_per_s"]}
+
+    if rank == 0:
+        line = {
+            "metric": "walk_steps_per_s", "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "m": int(len(src)),
+                       "weights": "loguniform[1,2^20)", "walks": n, "walk_len": WALK_LEN,
+                       "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}, "form": "plain (one launch per job)",
+                       "l2": "inputs larger than L2 (graph state and 320 MB walk output per step)",
+                       "parallelism": f"replicas x{world}"},
+            "walk_steps_per_s": steps_local / (walk_ms / 1e3),
+            "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * args.steps / (upd_ms / 1e3),
+            "e2e": {"value": e2e_steps / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches) * world,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-walks", type=int, default=131072)
+    ap.add_argument("--ref-walks", type=int, default=131072)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

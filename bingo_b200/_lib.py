@@ -1,0 +1,124 @@
+"""ctypes binding of libbingo.so (include/bingo.h, include/bingo_gen.h).
+
+The shared library is built in-tree (``make -C bingo_b200``). Importing this
+module raises if it is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_uint8, c_uint32, c_uint64, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbingo.so")
+
+
+class BingoConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", c_int32),
+        ("node2vec", c_uint32),
+        ("synchronous", c_uint32),
+        ("reserved0", c_uint32),
+        ("arena_factor", c_double),
+        ("arena_bytes", c_uint64),
+    ]
+
+
+class BingoWalkJob(ctypes.Structure):
+    _fields_ = [
+        ("app", c_int32),
+        ("length", c_uint32),
+        ("starts", c_void_p),
+        ("n_starts", c_uint64),
+        ("first", c_uint32),
+        ("job_id", c_uint32),
+        ("seed", c_uint64),
+        ("flags", c_uint32),
+        ("reserved0", c_uint32),
+        ("p", c_double),
+        ("q", c_double),
+        ("stop_prob", c_double),
+        ("out", c_void_p),
+    ]
+
+
+class BingoStats(ctypes.Structure):
+    _fields_ = [
+        ("n", c_uint32),
+        ("reserved0", c_uint32),
+        ("slots", c_uint64),
+        ("live_edges", c_uint64),
+        ("arena_bytes", c_uint64),
+        ("arena_used", c_uint64),
+        ("scratch_bytes", c_uint64),
+        ("walk_steps", c_uint64),
+        ("kernel_launches", c_uint64),
+    ]
+
+
+# Every symbol include/bingo.h and include/bingo_gen.h declare, with its
+# ctypes signature (restype, argtypes).
+SIGNATURES = {
+    "bingo_config_init": (None, [POINTER(BingoConfig)]),
+    "bingo_create": (c_int, [POINTER(BingoConfig), POINTER(c_void_p)]),
+    "bingo_destroy": (c_int, [c_void_p]),
+    "bingo_last_error": (c_char_p, [c_void_p]),
+    "bingo_load_edges": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_uint32]),
+    "bingo_insert_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
+    "bingo_delete_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
+    "bingo_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32, c_uint32]),
+    "bingo_sync": (c_int, [c_void_p]),
+    "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
+    "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),
+    "bingo_dump_sizes": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "bingo_dump_state": (c_int, [c_void_p] + [c_void_p] * 13),
+    "bingo_philox": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
+    "bingo_gen_rmat": (c_uint64, [c_uint32, c_uint32, c_double, c_double, c_double, c_uint64, c_void_p, c_void_p]),
+    "bingo_gen_weights": (None, [c_uint64, c_int, c_double, c_double, c_double, c_uint64, c_void_p]),
+    "bingo_updgen_create": (c_void_p, [c_uint32, c_void_p, c_void_p, c_uint64, c_uint64]),
+    "bingo_updgen_destroy": (None, [c_void_p]),
+    "bingo_updgen_inserts": (c_uint64, [c_void_p, c_uint64, c_int, c_double, c_double, c_double, c_void_p,
+                                        c_void_p, c_void_p]),
+    "bingo_updgen_deletes": (c_uint64, [c_void_p, c_uint64, c_void_p, c_void_p]),
+    "bingo_updgen_live": (c_uint64, [c_void_p]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbingo.so once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C bingo_b200` "
+                              "(the engine has no non-CUDA fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+STATUS = {
+    0: "BINGO_OK",
+    1: "BINGO_ERR_INVALID_ARGUMENT",
+    2: "BINGO_ERR_OUT_OF_RANGE",
+    3: "BINGO_ERR_ZERO_WEIGHT",
+    4: "BINGO_ERR_INVALID_SLOT",
+    5: "BINGO_ERR_CAPACITY",
+    6: "BINGO_ERR_CUDA",
+    7: "BINGO_ERR_NOT_LOADED",
+    8: "BINGO_ERR_TIMEOUT",
+    9: "BINGO_ERR_NO_DEVICE",
+    10: "BINGO_ERR_UNSUPPORTED",
+}
+
+
+class BingoError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))

@@ -1,0 +1,147 @@
+// extern "C" boundary: every entry point catches engine errors and returns a
+// bingo_status; the message stays readable through bingo_last_error().
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/bingo.h"
+#include "engine.cuh"
+
+struct bingo_handle {
+  bingo::Engine* eng = nullptr;
+  int device = 0;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(bingo_handle* h, F&& f) {
+  if (!h || !h->eng) return BINGO_ERR_INVALID_ARGUMENT;
+  try {
+    if (cudaSetDevice(h->device) != cudaSuccess) {
+      cudaGetLastError();
+      h->eng->last_error = "cudaSetDevice failed";
+      return BINGO_ERR_CUDA;
+    }
+    h->eng->last_error.clear();
+    f(*h->eng);
+    return BINGO_OK;
+  } catch (const bingo::Error& e) {
+    h->eng->last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    h->eng->last_error = "host allocation failed";
+    return BINGO_ERR_CAPACITY;
+  } catch (const std::exception& e) {
+    h->eng->last_error = e.what();
+    return BINGO_ERR_CUDA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void bingo_config_init(bingo_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof *cfg);
+  cfg->device = 0;
+  cfg->node2vec = 1;
+  cfg->synchronous = 1;
+  cfg->arena_factor = 2.0;
+  cfg->arena_bytes = 0;
+}
+
+int bingo_create(const bingo_config* cfg, bingo_handle** out) {
+  if (!out) return BINGO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  bingo_config c;
+  bingo_config_init(&c);
+  if (cfg) c = *cfg;
+  try {
+    bingo_handle* h = new bingo_handle;
+    h->device = c.device;
+    try {
+      h->eng = new bingo::Engine(c);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    g_create_error.clear();
+    return BINGO_OK;
+  } catch (const bingo::Error& e) {
+    g_create_error = e.what();
+    return e.status;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return BINGO_ERR_CUDA;
+  }
+}
+
+int bingo_destroy(bingo_handle* h) {
+  if (!h) return BINGO_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(h->device);
+  delete h->eng;
+  delete h;
+  return BINGO_OK;
+}
+
+const char* bingo_last_error(const bingo_handle* h) {
+  if (!h || !h->eng) return g_create_error.c_str();
+  return h->eng->last_error.c_str();
+}
+
+int bingo_load_edges(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m,
+                     uint32_t n) {
+  return guarded(h, [&](bingo::Engine& e) { e.load(src, dst, w, m, n); });
+}
+
+int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k,
+                       uint32_t* out_slots) {
+  return guarded(h, [&](bingo::Engine& e) { e.insert(src, dst, w, k, out_slots); });
+}
+
+int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot, uint64_t k) {
+  return guarded(h, [&](bingo::Engine& e) { e.erase(u, slot, k); });
+}
+
+int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
+  return guarded(h, [&](bingo::Engine& e) { e.walk(jobs, n_jobs, mode); });
+}
+
+int bingo_sync(bingo_handle* h) {
+  int st = BINGO_OK;
+  const int g = guarded(h, [&](bingo::Engine& e) { st = e.sync(); });
+  return g ? g : st;
+}
+
+int bingo_set_stream(bingo_handle* h, void* stream) {
+  return guarded(h, [&](bingo::Engine& e) { e.set_stream(stream); });
+}
+
+int bingo_get_stats(bingo_handle* h, bingo_stats* out) {
+  if (!out) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) { e.stats(out); });
+}
+
+int bingo_dump_sizes(bingo_handle* h, uint64_t sizes[3]) {
+  if (!sizes) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) { e.dump_sizes(sizes); });
+}
+
+int bingo_dump_state(bingo_handle* h, uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, uint32_t* gcnt,
+                     uint32_t* mslot, uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT,
+                     uint8_t* aown, uint8_t* aalias) {
+  return guarded(h, [&](bingo::Engine& e) {
+    e.dump(ecnt, live, ev, ew, gcnt, mslot, mv, mbp, am, athr, aT, aown, aalias);
+  });
+}
+
+int bingo_philox(bingo_handle* h, const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4) {
+  return guarded(h, [&](bingo::Engine& e) { e.philox_batch(ctr4, count, key, out4); });
+}
+
+}  // extern "C"

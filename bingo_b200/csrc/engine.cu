@@ -1,0 +1,904 @@
+// Engine: kernels and host orchestration for load / insert / delete / walk.
+//
+// Update batches run as: validate -> stable radix sort by vertex (CUB) ->
+// gather + segment heads -> segment list -> plan (per-vertex growth sizes) ->
+// exclusive scans per arena -> reserve -> apply (warp per vertex). Arena
+// offsets come from scans, so the layout is a deterministic function of the
+// inputs; arenas are index-addressed and grow by reallocation on the host
+// before a batch that would not fit.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.cuh"
+#include "store.cuh"
+#include "walk.cuh"
+
+namespace bingo {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr unsigned long long kUnitBytes[kArenas] = {4, sizeof(EdgeRec), 4, sizeof(AliasRec), sizeof(HashEntry)};
+// Index limits imposed by the 32-bit offsets in the walk-side records.
+constexpr unsigned long long kArenaLimit[kArenas] = {(1ull << 34), ~0ull, ~0ull, (1ull << 32), (1ull << 32)};
+constexpr unsigned long long kArenaFloor[kArenas] = {1024, 1024, 1024, 256, 1024};
+const char* const kArenaName[kArenas] = {"member", "edge", "back-pointer", "alias", "adjacency"};
+
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+unsigned grid_for(unsigned long long items, unsigned per_block, unsigned max_per_sm = 8) {
+  const unsigned long long want = (items + per_block - 1) / per_block;
+  const unsigned long long cap = (unsigned long long)sm_count() * max_per_sm;
+  return (unsigned)std::max(1ull, std::min(want, cap));
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_iota(uint32_t* a, unsigned long long n) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    a[i] = (uint32_t)i;
+}
+
+// Range / weight checks of a batch. Any bit set in ctl aborts the batch.
+__global__ void k_validate(const uint32_t* a, const uint32_t* b, const uint32_t* w, unsigned long long k, uint32_t n,
+                           uint32_t* ctl, uint32_t* err) {
+  uint32_t bits = 0;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    if (a[i] >= n || (b && b[i] >= n)) bits |= E_RANGE;
+    if (w && w[i] == 0u) bits |= E_ZERO_WEIGHT;
+  }
+  bits = __reduce_or_sync(kFull, bits);
+  if (bits && (threadIdx.x & 31) == 0) {
+    atomicOr(ctl, bits);
+    atomicOr(err, bits);
+  }
+}
+
+// Sorted order -> payload columns in sorted order + segment heads.
+__global__ void k_gather(const uint32_t* key, const uint32_t* perm, const uint32_t* a, const uint32_t* b,
+                         uint32_t* sa, uint32_t* sb, uint8_t* head, unsigned long long k) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t p = perm[i];
+    sa[i] = a[p];
+    if (b) sb[i] = b[p];
+    head[i] = (i == 0 || key[i] != key[i - 1]) ? 1 : 0;
+  }
+}
+
+__device__ __forceinline__ void seg_bounds(const uint32_t* seg, uint32_t S, uint32_t s, unsigned long long k,
+                                           uint32_t* b, uint32_t* e) {
+  *b = seg[s];
+  *e = s + 1 < S ? seg[s + 1] : (uint32_t)k;
+}
+
+// Per-segment arena sizes (need is [kArenas][ks], zero past the last segment).
+__global__ void k_plan(StoreView S, const uint32_t* skey, const uint32_t* sw, const uint32_t* seg,
+                       const uint32_t* nseg, unsigned long long k, uint32_t ks, const uint32_t* ctl,
+                       unsigned long long* need) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * blockDim.x / 32;
+  const uint32_t nS = *nseg;
+  const bool abort = *ctl != 0;
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < ks; s += warps) {
+    unsigned long long nd[kArenas] = {0, 0, 0, 0, 0};
+    if (!abort && s < nS) {
+      uint32_t b, e;
+      seg_bounds(seg, nS, s, k, &b, &e);
+      const uint32_t u = skey[b];
+      if (u < S.n) plan_append(S, u, sw + b, e - b, nd);
+    }
+    if (lane == 0)
+      for (int a = 0; a < kArenas; ++a) need[(size_t)a * ks + s] = nd[a];
+  }
+}
+
+__global__ void k_totals(const unsigned long long* need, const unsigned long long* scan, uint32_t ks,
+                         unsigned long long* tot) {
+  const int a = threadIdx.x;
+  if (a < kArenas) tot[a] = ks ? scan[(size_t)a * ks + ks - 1] + need[(size_t)a * ks + ks - 1] : 0;
+}
+
+// All-or-nothing reservation of the batch's arena space.
+__global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base) {
+  if (threadIdx.x || blockIdx.x || *ctl) return;
+  bool ok = true;
+  for (int a = 0; a < kArenas; ++a)
+    if (S.top[a] + tot[a] > S.cap[a]) ok = false;
+  if (!ok) {
+    atomicOr(ctl, E_CAPACITY);
+    atomicOr(S.err, E_CAPACITY);
+    return;
+  }
+  for (int a = 0; a < kArenas; ++a) {
+    base[a] = S.top[a];
+    S.top[a] += tot[a];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint32_t* skey, const uint32_t* sv,
+                                                         const uint32_t* sw, const uint32_t* sorig,
+                                                         const uint32_t* seg, const uint32_t* nseg,
+                                                         unsigned long long k, uint32_t ks, const uint32_t* ctl,
+                                                         const unsigned long long* scan,
+                                                         const unsigned long long* base, uint32_t* out_slots) {
+  if (*ctl) return;
+  const uint32_t warps = gridDim.x * blockDim.x / 32;
+  const uint32_t nS = *nseg;
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
+    uint32_t b, e;
+    seg_bounds(seg, nS, s, k, &b, &e);
+    const uint32_t u = skey[b];
+    if (u >= S.n) continue;
+    unsigned long long res[kArenas];
+#pragma unroll
+    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + scan[(size_t)a * ks + s];
+    apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
+                                                         const uint32_t* seg, const uint32_t* nseg,
+                                                         unsigned long long k, const uint32_t* ctl) {
+  if (*ctl) return;
+  const uint32_t warps = gridDim.x * blockDim.x / 32;
+  const uint32_t nS = *nseg;
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
+    uint32_t b, e;
+    seg_bounds(seg, nS, s, k, &b, &e);
+    const uint32_t u = skey[b];
+    if (u >= S.n) continue;
+    apply_delete(S, u, sslot + b, e - b);
+  }
+}
+
+template <int APP>
+__global__ void __launch_bounds__(kBlock) k_walk_plain(WalkView W, WalkJobDev J) {
+  unsigned long long steps = 0;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  // Uniform trip count across the warp so the closing shuffle sees all lanes.
+  const unsigned long long first = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u);
+  for (unsigned long long b = first; b < J.n; b += stride) {
+    const unsigned long long i = b + (threadIdx.x & 31);
+    if (i < J.n) steps += run_walk<APP>(W, J, (uint32_t)i);
+  }
+  add_steps(W, steps);
+}
+
+// Persistent walk kernel over a heterogeneous job list: warps pull 32 walks
+// at a time from one device counter (reset by the host before launch);
+// each lane decodes its own job by binary search over the walk prefix.
+__global__ void __launch_bounds__(kBlock) k_walk_batched(WalkView W, const WalkJobDev* jobs,
+                                                         const unsigned long long* prefix, uint32_t n_jobs,
+                                                         unsigned long long total, unsigned long long* queue) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long steps = 0;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32ull);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= total) break;
+    const unsigned long long item = base + lane;
+    if (item < total) {
+      uint32_t lo = 0, hi = n_jobs;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (prefix[mid] <= item)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const WalkJobDev J = jobs[lo];
+      steps += run_walk_any(W, J, (uint32_t)(item - prefix[lo]));
+    }
+  }
+  add_steps(W, steps);
+}
+
+__global__ void k_philox(const uint32_t* ctr, unsigned long long count, uint32_t k0, uint32_t k1, uint32_t* out) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < count;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const Rand4 r = philox(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3], k0, k1);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
+  }
+}
+
+uint64_t prob_threshold(double p) {
+  if (!(p > 0.0)) return 0;
+  if (p >= 1.0) return 1ull << 32;
+  const double t = std::floor(std::ldexp(p, 32));
+  return t >= 4294967296.0 ? (1ull << 32) : (uint64_t)t;
+}
+
+int status_of(uint32_t bits) {
+  if (bits & E_RANGE) return BINGO_ERR_OUT_OF_RANGE;
+  if (bits & E_ZERO_WEIGHT) return BINGO_ERR_ZERO_WEIGHT;
+  if (bits & E_CAPACITY) return BINGO_ERR_CAPACITY;
+  if (bits & E_INVALID_SLOT) return BINGO_ERR_INVALID_SLOT;
+  if (bits & E_TIMEOUT) return BINGO_ERR_TIMEOUT;
+  return BINGO_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ basics
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? BINGO_ERR_CAPACITY : BINGO_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+void DevBuf::ensure(size_t want, const char* what) {
+  if (want <= bytes && p) return;
+  release();
+  const size_t b = std::max(want, (size_t)256);
+  cuda_check(cudaMalloc(&p, b), what);
+  bytes = b;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    throw Error(BINGO_ERR_NO_DEVICE, "no CUDA device is available");
+  }
+  if (cfg.device < 0 || cfg.device >= count) throw Error(BINGO_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+  if (!(cfg.arena_factor >= 1.0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "arena_factor must be >= 1");
+  cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
+  cuda_check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  stream_ = own_stream_;
+  cuda_check(cudaMalloc(&d_err_, 4 * sizeof(uint32_t)), "cudaMalloc(err)");
+  cuda_check(cudaMemset(d_err_, 0, 4 * sizeof(uint32_t)), "memset(err)");
+  cuda_check(cudaMalloc(&d_top_, kArenas * sizeof(unsigned long long)), "cudaMalloc(top)");
+  cuda_check(cudaMalloc(&d_steps_, sizeof(unsigned long long)), "cudaMalloc(steps)");
+  cuda_check(cudaMemset(d_steps_, 0, sizeof(unsigned long long)), "memset(steps)");
+  cuda_check(cudaMemset(d_top_, 0, kArenas * sizeof(unsigned long long)), "memset(top)");
+  cuda_check(cudaMallocHost(&h_err_, 4 * sizeof(uint32_t)), "cudaMallocHost(err)");
+  cuda_check(cudaMallocHost(&h_top_, kArenas * sizeof(unsigned long long)), "cudaMallocHost(top)");
+  std::memset(h_top_, 0, kArenas * sizeof(unsigned long long));
+}
+
+Engine::~Engine() {
+  cudaSetDevice(cfg_.device);
+  if (stream_) cudaStreamSynchronize(stream_);
+  DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
+                    &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
+                    &prefix_, &queue_, &wstart_, &wout_};
+  for (DevBuf* b : bufs) b->release();
+  for (auto& a : arena_) a.release();
+  if (d_err_) cudaFree(d_err_);
+  if (d_top_) cudaFree(d_top_);
+  if (d_steps_) cudaFree(d_steps_);
+  if (h_err_) cudaFreeHost(h_err_);
+  if (h_top_) cudaFreeHost(h_top_);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+StoreView Engine::view() const {
+  StoreView S;
+  S.n = n_;
+  S.vrec = vrec_.as<VertexRec>();
+  S.meta = meta_.as<VertexMeta>();
+  S.gdesc = gdesc_.as<GroupDesc>();
+  S.gv = arena_[A_MEMBER].as<uint32_t>();
+  S.gs = gs_.as<uint32_t>();
+  S.edges = arena_[A_EDGE].as<EdgeRec>();
+  S.bp = arena_[A_BP].as<uint32_t>();
+  S.alias = arena_[A_ALIAS].as<AliasRec>();
+  S.hash = arena_[A_HASH].as<HashEntry>();
+  S.top = d_top_;
+  for (int a = 0; a < kArenas; ++a) S.cap[a] = cap_[a];
+  S.err = d_err_;
+  S.node2vec = cfg_.node2vec;
+  return S;
+}
+
+WalkView Engine::wview() const {
+  WalkView W;
+  W.n = n_;
+  W.vrec = vrec_.as<VertexRec>();
+  W.alias = arena_[A_ALIAS].as<AliasRec>();
+  W.gv = arena_[A_MEMBER].as<uint32_t>();
+  W.hash = arena_[A_HASH].as<HashEntry>();
+  W.err = d_err_;
+  W.steps = d_steps_;
+  return W;
+}
+
+void Engine::require_loaded() const {
+  if (!loaded_) throw Error(BINGO_ERR_NOT_LOADED, "no graph loaded");
+}
+
+void Engine::set_stream(void* s) { stream_ = s ? (cudaStream_t)s : own_stream_; }
+
+int Engine::sync() {
+  cuda_check(cudaStreamSynchronize(stream_), "stream synchronize");
+  cuda_check(cudaMemcpy(h_err_, d_err_, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost), "read status");
+  const uint32_t bits = h_err_[0], rejected = h_err_[1];
+  if (!bits) return BINGO_OK;
+  cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
+  const int st = status_of(bits);
+  last_error = "device reported error bits 0x" + std::to_string(bits);
+  if (bits & E_INVALID_SLOT) last_error += " (" + std::to_string(rejected) + " deletes of absent slots skipped)";
+  if (bits & E_RANGE) last_error += " (vertex id out of range)";
+  if (bits & E_ZERO_WEIGHT) last_error += " (zero weight)";
+  return st;
+}
+
+void Engine::finish_call() {
+  if (!cfg_.synchronous) return;
+  const int st = sync();
+  if (st) throw Error(st, last_error);
+}
+
+// ------------------------------------------------------------------ staging
+void Engine::ensure_batch_scratch(uint64_t k) {
+  const uint64_t kk = std::max<uint64_t>(k, 1);
+  const uint64_t ks = std::max<uint64_t>(std::min<uint64_t>(kk, n_ ? n_ : kk), 1);
+  in_a_.ensure(kk * 4, "scratch");
+  in_b_.ensure(kk * 4, "scratch");
+  in_c_.ensure(kk * 4, "scratch");
+  key_s_.ensure(kk * 4, "scratch");
+  perm_.ensure(kk * 4, "scratch");
+  sa_.ensure(kk * 4, "scratch");
+  sb_.ensure(kk * 4, "scratch");
+  head_.ensure(kk, "scratch");
+  seg_.ensure(kk * 4, "scratch");
+  slots_.ensure(kk * 4, "scratch");
+  nseg_.ensure(16, "scratch");
+  ctl_.ensure(16, "scratch");
+  base_.ensure(kArenas * 8 * 2, "scratch");
+  need_.ensure((size_t)kArenas * ks * 8, "scratch");
+  scan_.ensure((size_t)kArenas * ks * 8, "scratch");
+  if (iota_n_ < kk) {
+    iota_.ensure(kk * 4, "scratch");
+    k_iota<<<grid_for(kk, kBlock), kBlock, 0, stream_>>>(iota_.as<uint32_t>(), kk);
+    cuda_check(cudaGetLastError(), "iota");
+    ++launches_;
+    iota_n_ = kk;
+  }
+  size_t t_sort = 0, t_sel = 0, t_scan = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)kk, 0, 32, stream_);
+  cub::DeviceSelect::Flagged(nullptr, t_sel, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
+                             (uint32_t*)nullptr, (int)kk, stream_);
+  cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                (int)ks, stream_);
+  cub_tmp_.ensure(std::max(t_sort, std::max(t_sel, t_scan)), "scratch");
+}
+
+const uint32_t* Engine::stage(const uint32_t* p, uint64_t k, DevBuf& buf, const char* what) {
+  if (!p) return nullptr;
+  if (is_device_ptr(p)) return p;
+  cuda_check(cudaMemcpyAsync(buf.p, p, k * 4, cudaMemcpyHostToDevice, stream_), what);
+  return buf.as<uint32_t>();
+}
+
+// Stable sort of the batch by vertex; leaves sorted keys in key_s_, the
+// original index in perm_, payloads a/b in sorted order in sa_/sb_, and the
+// segment start list in seg_ with its count in nseg_.
+void Engine::group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k) {
+  int end_bit = 1;
+  while (end_bit < 32 && (1ull << end_bit) < n_) ++end_bit;
+  size_t tb = cub_tmp_.bytes;
+  cuda_check(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tb, key, key_s_.as<uint32_t>(), iota_.as<uint32_t>(),
+                                             perm_.as<uint32_t>(), (int)k, 0, end_bit, stream_),
+             "radix sort");
+  k_gather<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(key_s_.as<uint32_t>(), perm_.as<uint32_t>(), a, b,
+                                                             sa_.as<uint32_t>(), sb_.as<uint32_t>(),
+                                                             head_.as<uint8_t>(), k);
+  cuda_check(cudaGetLastError(), "gather");
+  ++launches_;
+  tb = cub_tmp_.bytes;
+  cuda_check(cub::DeviceSelect::Flagged(cub_tmp_.p, tb, iota_.as<uint32_t>(), head_.as<uint8_t>(),
+                                        seg_.as<uint32_t>(), nseg_.as<uint32_t>(), (int)k, stream_),
+             "segment select");
+}
+
+void Engine::read_tops() {
+  cuda_check(cudaMemcpyAsync(h_top_, d_top_, kArenas * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+             "read tops");
+  cuda_check(cudaStreamSynchronize(stream_), "read tops");
+}
+
+void Engine::grow_arena(int a, unsigned long long min_cap) {
+  unsigned long long nc = std::max<unsigned long long>(min_cap, cap_[a] + cap_[a] / 2);
+  nc = std::min(nc, kArenaLimit[a]);
+  if (nc < min_cap)
+    throw Error(BINGO_ERR_CAPACITY, std::string(kArenaName[a]) + " arena would exceed its 32-bit index range");
+  const unsigned long long used = h_top_[a];
+  DevBuf fresh;
+  fresh.ensure(nc * kUnitBytes[a], "grow arena");
+  if (used) cuda_check(cudaMemcpyAsync(fresh.p, arena_[a].p, used * kUnitBytes[a], cudaMemcpyDeviceToDevice, stream_),
+                       "grow arena copy");
+  if (a == A_MEMBER) {
+    DevBuf fgs;
+    fgs.ensure(nc * 4, "grow arena");
+    if (used) cuda_check(cudaMemcpyAsync(fgs.p, gs_.p, used * 4, cudaMemcpyDeviceToDevice, stream_), "grow copy");
+    cuda_check(cudaStreamSynchronize(stream_), "grow arena");
+    gs_.release();
+    gs_ = fgs;
+    fgs.p = nullptr;
+  }
+  cuda_check(cudaStreamSynchronize(stream_), "grow arena");
+  arena_[a].release();
+  arena_[a] = fresh;
+  fresh.p = nullptr;
+  cap_[a] = nc;
+}
+
+void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
+  for (int a = 0; a < kArenas; ++a) {
+    if (a == A_HASH && !cfg_.node2vec) {
+      cap_[a] = 0;
+      arena_[a].ensure(256, "arena");
+      continue;
+    }
+    unsigned long long c = (unsigned long long)std::ceil((double)need[a] * cfg_.arena_factor);
+    c = std::max(c, need[a] + kArenaFloor[a]);
+    c = std::min(c, kArenaLimit[a]);
+    if (c < need[a]) throw Error(BINGO_ERR_CAPACITY, std::string(kArenaName[a]) + " arena exceeds its index range");
+    arena_[a].release();
+    arena_[a].ensure(c * kUnitBytes[a], "allocate arena");
+    if (a == A_MEMBER) {
+      gs_.release();
+      gs_.ensure(c * 4, "allocate arena");
+    }
+    cap_[a] = c;
+  }
+  if (cfg_.arena_bytes) {
+    // Spread an explicit minimum over the arenas in proportion to their need.
+    unsigned long long total = 0;
+    for (int a = 0; a < kArenas; ++a) total += cap_[a] * kUnitBytes[a] + (a == A_MEMBER ? cap_[a] * 4 : 0);
+    if (total < cfg_.arena_bytes) {
+      const double scale = (double)cfg_.arena_bytes / (double)std::max<unsigned long long>(total, 1);
+      for (int a = 0; a < kArenas; ++a)
+        if (cap_[a]) grow_arena(a, (unsigned long long)std::ceil(cap_[a] * scale));
+    }
+  }
+  cuda_check(cudaMemsetAsync(d_top_, 0, kArenas * sizeof(unsigned long long), stream_), "reset tops");
+  std::memset(h_top_, 0, kArenas * sizeof(unsigned long long));
+}
+
+// Plan, size, reserve and apply an append batch whose grouped columns are in
+// key_s_/sa_ (dst)/sb_ (w)/perm_ (original index) and segments in seg_/nseg_.
+void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t) {
+  const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
+  const StoreView S0 = view();
+  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
+      S0, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
+      ctl_.as<uint32_t>(), need_.as<unsigned long long>());
+  cuda_check(cudaGetLastError(), "plan");
+  ++launches_;
+  for (int a = 0; a < kArenas; ++a) {
+    size_t tb = cub_tmp_.bytes;
+    cuda_check(cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tb, need_.as<unsigned long long>() + (size_t)a * ks,
+                                             scan_.as<unsigned long long>() + (size_t)a * ks, (int)ks, stream_),
+               "scan");
+  }
+  unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
+  k_totals<<<1, 32, 0, stream_>>>(need_.as<unsigned long long>(), scan_.as<unsigned long long>(), ks, d_tot);
+  cuda_check(cudaGetLastError(), "totals");
+  ++launches_;
+  unsigned long long tot[kArenas];
+  uint32_t ctl = 0;
+  cuda_check(cudaMemcpyAsync(tot, d_tot, sizeof tot, cudaMemcpyDeviceToHost, stream_), "read totals");
+  cuda_check(cudaMemcpyAsync(&ctl, ctl_.p, 4, cudaMemcpyDeviceToHost, stream_), "read ctl");
+  cuda_check(cudaStreamSynchronize(stream_), "plan sync");
+  if (ctl) {
+    cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
+    const int st = status_of(ctl);
+    throw Error(st, st == BINGO_ERR_ZERO_WEIGHT ? "batch holds a zero weight" : "batch holds a vertex id >= n");
+  }
+  if (load_mode) {
+    alloc_arenas(tot);
+  } else {
+    for (int a = 0; a < kArenas; ++a)
+      if (h_top_[a] + tot[a] > cap_[a]) grow_arena(a, h_top_[a] + tot[a]);
+  }
+  const StoreView S = view();
+  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
+  cuda_check(cudaGetLastError(), "reserve");
+  ++launches_;
+  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+      S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
+      base_.as<unsigned long long>(), dev_out_slots);
+  cuda_check(cudaGetLastError(), "apply insert");
+  ++launches_;
+  for (int a = 0; a < kArenas; ++a) h_top_[a] += tot[a];
+}
+
+// ------------------------------------------------------------------ API ops
+namespace {
+void host_check_ids(const uint32_t* a, uint64_t k, uint32_t n, const char* what) {
+  for (uint64_t i = 0; i < k; ++i)
+    if (a[i] >= n) throw Error(BINGO_ERR_OUT_OF_RANGE, std::string(what) + " id " + std::to_string(a[i]) + " >= n");
+}
+void host_check_weights(const uint32_t* w, uint64_t k) {
+  for (uint64_t i = 0; i < k; ++i)
+    if (w[i] == 0) throw Error(BINGO_ERR_ZERO_WEIGHT, "weight 0 at index " + std::to_string(i));
+}
+}  // namespace
+
+void Engine::load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n) {
+  if (n == 0) throw Error(BINGO_ERR_INVALID_ARGUMENT, "n must be > 0");
+  if (m && (!src || !dst || !w)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null edge array");
+  if (m >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 edges in one load");
+  if (m && !is_device_ptr(src)) host_check_ids(src, m, n, "source");
+  if (m && !is_device_ptr(dst)) host_check_ids(dst, m, n, "destination");
+  if (m && !is_device_ptr(w)) host_check_weights(w, m);
+  cuda_check(cudaStreamSynchronize(stream_), "load");
+  loaded_ = false;
+  n_ = n;
+  vrec_.release(), meta_.release(), gdesc_.release();
+  vrec_.ensure((size_t)n * sizeof(VertexRec), "vertex records");
+  meta_.ensure((size_t)n * sizeof(VertexMeta), "vertex metadata");
+  gdesc_.ensure((size_t)n * kBits * sizeof(GroupDesc), "group descriptors");
+  cuda_check(cudaMemsetAsync(vrec_.p, 0, (size_t)n * sizeof(VertexRec), stream_), "memset");
+  cuda_check(cudaMemsetAsync(meta_.p, 0, (size_t)n * sizeof(VertexMeta), stream_), "memset");
+  cuda_check(cudaMemsetAsync(gdesc_.p, 0, (size_t)n * kBits * sizeof(GroupDesc), stream_), "memset");
+  for (int a = 0; a < kArenas; ++a) arena_[a].release(), cap_[a] = 0;
+  gs_.release();
+  cuda_check(cudaMemsetAsync(d_top_, 0, kArenas * sizeof(unsigned long long), stream_), "reset tops");
+  std::memset(h_top_, 0, kArenas * sizeof(unsigned long long));
+  if (m == 0) {
+    const unsigned long long zero[kArenas] = {0, 0, 0, 0, 0};
+    alloc_arenas(zero);
+    loaded_ = true;
+    finish_call();
+    return;
+  }
+  ensure_batch_scratch(m);
+  const uint32_t* ds = stage(src, m, in_a_, "stage src");
+  const uint32_t* dd = stage(dst, m, in_b_, "stage dst");
+  const uint32_t* dw = stage(w, m, in_c_, "stage w");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(m, kBlock, 16), kBlock, 0, stream_>>>(ds, dd, dw, m, n, ctl_.as<uint32_t>(), d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  group_by_vertex(ds, dd, dw, m);
+  run_insert(m, nullptr, true, m);
+  loaded_ = true;
+  // Release load-sized scratch; update batches re-grow what they need.
+  DevBuf* big[] = {&in_a_, &in_b_, &in_c_, &key_s_, &perm_, &sa_, &sb_, &head_, &seg_, &slots_, &need_,
+                   &scan_, &iota_, &cub_tmp_};
+  cuda_check(cudaStreamSynchronize(stream_), "load");
+  for (DevBuf* b : big) b->release();
+  iota_n_ = 0;
+  finish_call();
+}
+
+void Engine::insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots) {
+  require_loaded();
+  if (k == 0) return;
+  if (!src || !dst || !w) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null edge array");
+  if (k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 edges in one batch");
+  if (!is_device_ptr(src)) host_check_ids(src, k, n_, "source");
+  if (!is_device_ptr(dst)) host_check_ids(dst, k, n_, "destination");
+  if (!is_device_ptr(w)) host_check_weights(w, k);
+  ensure_batch_scratch(k);
+  const uint32_t* ds = stage(src, k, in_a_, "stage src");
+  const uint32_t* dd = stage(dst, k, in_b_, "stage dst");
+  const uint32_t* dw = stage(w, k, in_c_, "stage w");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(ds, dd, dw, k, n_, ctl_.as<uint32_t>(), d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  group_by_vertex(ds, dd, dw, k);
+  const bool dev_out = out_slots && is_device_ptr(out_slots);
+  uint32_t* dslots = out_slots ? (dev_out ? out_slots : slots_.as<uint32_t>()) : nullptr;
+  run_insert(k, dslots, false, k);
+  if (out_slots && !dev_out)
+    cuda_check(cudaMemcpyAsync(out_slots, dslots, k * 4, cudaMemcpyDeviceToHost, stream_), "slots D2H");
+  finish_call();
+}
+
+void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
+  require_loaded();
+  if (k == 0) return;
+  if (!u || !slot) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null delete array");
+  if (k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 deletes in one batch");
+  if (!is_device_ptr(u)) host_check_ids(u, k, n_, "vertex");
+  ensure_batch_scratch(k);
+  const uint32_t* du = stage(u, k, in_a_, "stage u");
+  const uint32_t* dsl = stage(slot, k, in_b_, "stage slot");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, nullptr, nullptr, k, n_, ctl_.as<uint32_t>(),
+                                                              d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  group_by_vertex(du, dsl, nullptr, k);
+  const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
+  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+      view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
+      ctl_.as<uint32_t>());
+  cuda_check(cudaGetLastError(), "apply delete");
+  ++launches_;
+  finish_call();
+}
+
+void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
+  require_loaded();
+  if (n_jobs == 0) return;
+  if (!jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
+  if (mode != BINGO_WALK_BATCHED && mode != BINGO_WALK_PLAIN) throw Error(BINGO_ERR_INVALID_ARGUMENT, "bad mode");
+  std::vector<WalkJobDev> dj(n_jobs);
+  std::vector<unsigned long long> prefix(n_jobs + 1, 0);
+  // staging layout for host starts / outputs
+  std::vector<uint64_t> s_off(n_jobs, ~0ull), o_off(n_jobs, ~0ull);
+  uint64_t s_total = 0, o_total = 0;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const bingo_walk_job& J = jobs[j];
+    if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
+    if (J.app == BINGO_NODE2VEC && !cfg_.node2vec)
+      throw Error(BINGO_ERR_UNSUPPORTED, "node2vec needs the adjacency index (config.node2vec)");
+    if (J.app == BINGO_NODE2VEC && !(J.p > 0 && J.q > 0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "p, q must be > 0");
+    if (J.app == BINGO_PPR && !(J.stop_prob >= 0 && J.stop_prob <= 1))
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "stop_prob must be in [0, 1]");
+    if (J.app != BINGO_SAMPLING && J.length == 0 && J.n_starts)
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "length must be >= 1");
+    if (J.n_starts && !J.out) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null output");
+    if (J.n_starts >= (1ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one job");
+    if (J.starts) {
+      if (!is_device_ptr(J.starts)) {
+        host_check_ids(J.starts, J.n_starts, n_, "start");
+        s_off[j] = s_total;
+        s_total += J.n_starts;
+      }
+    } else if ((uint64_t)J.first + J.n_starts > n_) {
+      throw Error(BINGO_ERR_OUT_OF_RANGE, "start range exceeds n");
+    }
+    const uint64_t per = J.app == BINGO_SAMPLING ? 1 : J.length;
+    if (J.n_starts && !is_device_ptr(J.out)) {
+      o_off[j] = o_total;
+      o_total += J.n_starts * per;
+    }
+    prefix[j + 1] = prefix[j] + J.n_starts;
+  }
+  if (s_total) wstart_.ensure(s_total * 4, "walk staging");
+  if (o_total) wout_.ensure(o_total * 4, "walk staging");
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const bingo_walk_job& J = jobs[j];
+    WalkJobDev& D = dj[j];
+    D.app = J.app;
+    D.L = J.length;
+    D.n = J.n_starts;
+    D.first = J.first;
+    D.job = J.job_id;
+    D.k0 = (uint32_t)J.seed;
+    D.k1 = (uint32_t)(J.seed >> 32);
+    D.flags = J.flags;
+    D.pad = 0;
+    const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
+    const double wmax = std::max(wr, std::max(1.0, wo));
+    D.thr_ret = prob_threshold(wr / wmax);
+    D.thr_in = prob_threshold(1.0 / wmax);
+    D.thr_out = prob_threshold(wo / wmax);
+    D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+    D.starts = J.starts;
+    if (s_off[j] != ~0ull) {
+      uint32_t* d = wstart_.as<uint32_t>() + s_off[j];
+      cuda_check(cudaMemcpyAsync(d, J.starts, J.n_starts * 4, cudaMemcpyHostToDevice, stream_), "starts H2D");
+      D.starts = d;
+    }
+    D.out = o_off[j] != ~0ull ? wout_.as<int32_t>() + o_off[j] : J.out;
+  }
+  const WalkView W = wview();
+  if (mode == BINGO_WALK_PLAIN) {
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+      if (!dj[j].n) continue;
+      const unsigned g = grid_for(dj[j].n, kBlock, 8);
+      switch (dj[j].app) {
+        case APP_DEEPWALK: k_walk_plain<APP_DEEPWALK><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
+        case APP_NODE2VEC: k_walk_plain<APP_NODE2VEC><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
+        case APP_PPR: k_walk_plain<APP_PPR><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
+        default: k_walk_plain<APP_SAMPLING><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
+      }
+      cuda_check(cudaGetLastError(), "walk launch");
+  ++launches_;
+    }
+  } else if (prefix[n_jobs]) {
+    jobs_.ensure(n_jobs * sizeof(WalkJobDev), "walk jobs");
+    prefix_.ensure((n_jobs + 1) * 8, "walk jobs");
+    queue_.ensure(8, "walk queue");
+    cuda_check(cudaMemcpyAsync(jobs_.p, dj.data(), n_jobs * sizeof(WalkJobDev), cudaMemcpyHostToDevice, stream_),
+               "jobs H2D");
+    cuda_check(cudaMemcpyAsync(prefix_.p, prefix.data(), (n_jobs + 1) * 8, cudaMemcpyHostToDevice, stream_),
+               "prefix H2D");
+    cuda_check(cudaMemsetAsync(queue_.p, 0, 8, stream_), "queue reset");
+    const unsigned g = grid_for(prefix[n_jobs], kBlock, 8);
+    k_walk_batched<<<g, kBlock, 0, stream_>>>(W, jobs_.as<WalkJobDev>(), prefix_.as<unsigned long long>(), n_jobs,
+                                               prefix[n_jobs], queue_.as<unsigned long long>());
+    cuda_check(cudaGetLastError(), "walk launch");
+  ++launches_;
+  }
+  for (uint32_t j = 0; j < n_jobs; ++j)
+    if (o_off[j] != ~0ull) {
+      const uint64_t per = jobs[j].app == BINGO_SAMPLING ? 1 : jobs[j].length;
+      cuda_check(cudaMemcpyAsync(jobs[j].out, wout_.as<int32_t>() + o_off[j], jobs[j].n_starts * per * 4,
+                                 cudaMemcpyDeviceToHost, stream_),
+                 "walk D2H");
+    }
+  finish_call();
+}
+
+void Engine::philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4) {
+  if (!count) return;
+  if (!ctr4 || !out4) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null array");
+  DevBuf c, o;
+  c.ensure(count * 16, "philox");
+  o.ensure(count * 16, "philox");
+  cuda_check(cudaMemcpyAsync(c.p, ctr4, count * 16, cudaMemcpyDefault, stream_), "philox H2D");
+  k_philox<<<grid_for(count, kBlock), kBlock, 0, stream_>>>(c.as<uint32_t>(), count, (uint32_t)key,
+                                                           (uint32_t)(key >> 32), o.as<uint32_t>());
+  cuda_check(cudaGetLastError(), "philox");
+  ++launches_;
+  cuda_check(cudaMemcpyAsync(out4, o.p, count * 16, cudaMemcpyDefault, stream_), "philox D2H");
+  cuda_check(cudaStreamSynchronize(stream_), "philox");
+  c.release();
+  o.release();
+}
+
+// ------------------------------------------------------------------ state access
+void Engine::stats(bingo_stats* out) {
+  std::memset(out, 0, sizeof *out);
+  out->n = n_;
+  cuda_check(cudaStreamSynchronize(stream_), "stats");
+  cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
+  out->kernel_launches = launches_;
+  if (!loaded_) return;
+  read_tops();
+  std::vector<VertexMeta> meta(n_);
+  cuda_check(cudaMemcpy(meta.data(), meta_.p, (size_t)n_ * sizeof(VertexMeta), cudaMemcpyDeviceToHost), "stats");
+  for (const auto& M : meta) out->slots += M.ecnt, out->live_edges += M.live;
+  for (int a = 0; a < kArenas; ++a) {
+    out->arena_bytes += cap_[a] * kUnitBytes[a] + (a == A_MEMBER ? cap_[a] * 4 : 0);
+    out->arena_used += h_top_[a] * kUnitBytes[a] + (a == A_MEMBER ? h_top_[a] * 4 : 0);
+  }
+  const DevBuf* sc[] = {&in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_, &sb_, &head_, &seg_, &nseg_,
+                        &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_, &prefix_, &queue_, &wstart_,
+                        &wout_};
+  for (const DevBuf* b : sc) out->scratch_bytes += b->bytes;
+}
+
+namespace {
+struct HostState {
+  std::vector<VertexMeta> meta;
+  std::vector<GroupDesc> gd;
+  std::vector<VertexRec> vr;
+  std::vector<uint32_t> gv, gs, bp;
+  std::vector<EdgeRec> edges;
+  std::vector<AliasRec> alias;
+};
+}  // namespace
+
+static void fetch(HostState& H, uint32_t n, const DevBuf& meta, const DevBuf& gd, const DevBuf& vr,
+                  const DevBuf* arena, const DevBuf& gs, const unsigned long long* top) {
+  H.meta.resize(n);
+  H.gd.resize((size_t)n * kBits);
+  H.vr.resize(n);
+  cuda_check(cudaMemcpy(H.meta.data(), meta.p, (size_t)n * sizeof(VertexMeta), cudaMemcpyDeviceToHost), "dump");
+  cuda_check(cudaMemcpy(H.gd.data(), gd.p, H.gd.size() * sizeof(GroupDesc), cudaMemcpyDeviceToHost), "dump");
+  cuda_check(cudaMemcpy(H.vr.data(), vr.p, (size_t)n * sizeof(VertexRec), cudaMemcpyDeviceToHost), "dump");
+  H.gv.resize(top[A_MEMBER]);
+  H.gs.resize(top[A_MEMBER]);
+  H.edges.resize(top[A_EDGE]);
+  H.bp.resize(top[A_BP]);
+  H.alias.resize(top[A_ALIAS]);
+  if (top[A_MEMBER]) {
+    cuda_check(cudaMemcpy(H.gv.data(), arena[A_MEMBER].p, top[A_MEMBER] * 4, cudaMemcpyDeviceToHost), "dump");
+    cuda_check(cudaMemcpy(H.gs.data(), gs.p, top[A_MEMBER] * 4, cudaMemcpyDeviceToHost), "dump");
+  }
+  if (top[A_EDGE])
+    cuda_check(cudaMemcpy(H.edges.data(), arena[A_EDGE].p, top[A_EDGE] * sizeof(EdgeRec), cudaMemcpyDeviceToHost),
+               "dump");
+  if (top[A_BP]) cuda_check(cudaMemcpy(H.bp.data(), arena[A_BP].p, top[A_BP] * 4, cudaMemcpyDeviceToHost), "dump");
+  if (top[A_ALIAS])
+    cuda_check(
+        cudaMemcpy(H.alias.data(), arena[A_ALIAS].p, top[A_ALIAS] * sizeof(AliasRec), cudaMemcpyDeviceToHost),
+        "dump");
+}
+
+void Engine::dump_sizes(uint64_t sizes[3]) {
+  require_loaded();
+  cuda_check(cudaStreamSynchronize(stream_), "dump");
+  std::vector<VertexMeta> meta(n_);
+  std::vector<GroupDesc> gd((size_t)n_ * kBits);
+  std::vector<VertexRec> vr(n_);
+  cuda_check(cudaMemcpy(meta.data(), meta_.p, (size_t)n_ * sizeof(VertexMeta), cudaMemcpyDeviceToHost), "dump");
+  cuda_check(cudaMemcpy(gd.data(), gdesc_.p, gd.size() * sizeof(GroupDesc), cudaMemcpyDeviceToHost), "dump");
+  cuda_check(cudaMemcpy(vr.data(), vrec_.p, (size_t)n_ * sizeof(VertexRec), cudaMemcpyDeviceToHost), "dump");
+  uint64_t s = 0, mem = 0, a = 0;
+  for (uint32_t u = 0; u < n_; ++u) {
+    s += meta[u].ecnt;
+    for (int k = 0; k < kBits; ++k) mem += gd[(size_t)u * kBits + k].cnt;
+    a += vr[u].m;
+  }
+  sizes[0] = s, sizes[1] = mem, sizes[2] = a;
+}
+
+void Engine::dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, uint32_t* gcnt, uint32_t* mslot,
+                  uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT, uint8_t* aown,
+                  uint8_t* aalias) {
+  require_loaded();
+  read_tops();
+  HostState H;
+  fetch(H, n_, meta_, gdesc_, vrec_, arena_, gs_, h_top_);
+  uint64_t s = 0, mem = 0, a = 0;
+  for (uint32_t u = 0; u < n_; ++u) {
+    const VertexMeta& M = H.meta[u];
+    ecnt[u] = M.ecnt;
+    live[u] = M.live;
+    for (uint32_t i = 0; i < M.ecnt; ++i, ++s) {
+      const EdgeRec& e = H.edges[M.eoff + i];
+      ev[s] = e.v;
+      ew[s] = e.w;
+    }
+    for (int k = 0; k < kBits; ++k) {
+      const GroupDesc& G = H.gd[(size_t)u * kBits + k];
+      gcnt[(size_t)u * kBits + k] = G.cnt;
+      for (uint32_t p = 0; p < G.cnt; ++p, ++mem) {
+        const size_t idx = (size_t)G.base * 4 + p;
+        const uint32_t sl = H.gs[idx];
+        mslot[mem] = sl;
+        mv[mem] = H.gv[idx];
+        const EdgeRec& e = H.edges[M.eoff + sl];
+        mbp[mem] = H.bp[M.bpoff + e.ebp + __builtin_popcount(e.w & ((1u << k) - 1u))];
+      }
+    }
+    const VertexRec& R = H.vr[u];
+    am[u] = R.m;
+    int nzbits[kBits], nnz = 0;
+    for (int k = 0; k < kBits; ++k)
+      if (H.gd[(size_t)u * kBits + k].cnt) nzbits[nnz++] = k;
+    for (uint32_t j = 0; j < R.m; ++j, ++a) {
+      const AliasRec& A = H.alias[R.aoff + j];
+      athr[a] = A.thr;
+      aT[a] = A.T;
+      aown[a] = j < (uint32_t)nnz ? (uint8_t)nzbits[j] : 255;
+      uint8_t alt = 255;
+      for (int k = 0; k < kBits; ++k) {
+        const GroupDesc& G = H.gd[(size_t)u * kBits + k];
+        if (G.cnt && G.base == A.alt_base && G.cnt == A.alt_cnt) alt = (uint8_t)k;
+      }
+      aalias[a] = alt;
+    }
+  }
+}
+
+}  // namespace bingo

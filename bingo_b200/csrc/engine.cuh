@@ -1,0 +1,97 @@
+// Host-side engine behind the C ABI: owns the device graph store, the
+// staging buffers and the per-batch pipelines (group by vertex, plan, reserve,
+// apply) and launches the walk kernels.
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/bingo.h"
+#include "common.cuh"
+#include "walk.cuh"
+
+namespace bingo {
+
+// Error carrying a bingo_status across the engine; the C ABI turns it into
+// the return code and bingo_last_error().
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Device buffer that grows by reallocation (contents not preserved).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t want, const char* what);
+  void release();
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+class Engine {
+ public:
+  explicit Engine(const bingo_config& cfg);
+  ~Engine();
+
+  void load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n);
+  void insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
+  void erase(const uint32_t* u, const uint32_t* slot, uint64_t k);
+  void walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
+  int sync();  // returns a bingo_status
+  void set_stream(void* s);
+  void stats(bingo_stats* out);
+  void dump_sizes(uint64_t sizes[3]);
+  void dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, uint32_t* gcnt, uint32_t* mslot,
+            uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT, uint8_t* aown,
+            uint8_t* aalias);
+  void philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
+
+  std::string last_error;
+
+ private:
+  bingo_config cfg_;
+  cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
+  bool loaded_ = false;
+  uint32_t n_ = 0;
+
+  // store
+  DevBuf vrec_, meta_, gdesc_;
+  DevBuf arena_[kArenas];
+  DevBuf gs_;  // slot ids, parallel to the member arena
+  unsigned long long* d_top_ = nullptr;  // [kArenas]
+  unsigned long long cap_[kArenas] = {};
+  uint32_t* d_err_ = nullptr;            // [0] ErrBit sticky, [1] rejected deletes
+  uint32_t* h_err_ = nullptr;            // pinned mirror
+  unsigned long long* h_top_ = nullptr;  // pinned mirror of d_top_
+  unsigned long long* d_steps_ = nullptr;  // produced walk steps since create
+  unsigned long long launches_ = 0;        // hand-written kernels launched since create
+
+  // per-batch scratch
+  DevBuf in_a_, in_b_, in_c_, key_s_, perm_, iota_, sa_, sb_, head_, seg_, nseg_, need_, scan_, base_, ctl_,
+      slots_, cub_tmp_;
+  uint64_t iota_n_ = 0;
+  // walk scratch
+  DevBuf jobs_, prefix_, queue_, wstart_, wout_;
+
+  StoreView view() const;
+  WalkView wview() const;
+  void ensure_batch_scratch(uint64_t k);
+  const uint32_t* stage(const uint32_t* p, uint64_t k, DevBuf& buf, const char* what);
+  void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k);
+  void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
+  void alloc_arenas(const unsigned long long need[kArenas]);
+  void grow_arena(int a, unsigned long long min_cap);
+  void read_tops();
+  void finish_call();
+  void require_loaded() const;
+};
+
+bool is_device_ptr(const void* p);
+
+}  // namespace bingo

@@ -1,0 +1,351 @@
+// Warp-cooperative operations on the graph store. One warp owns one vertex;
+// lane k owns weight bit k (group k) for the whole operation.
+#pragma once
+#include "common.cuh"
+
+namespace bingo {
+
+// ---------------------------------------------------------------------------
+// Integer Vose alias table over the vertex's nonzero groups (lane k = group k).
+//
+// Slot j belongs to the j-th nonzero group in ascending bit order. Scaled
+// mass s_k = (cnt_k << k) * m, each slot holds exactly T scaled units. The
+// pairing always takes the lowest small (s < T) and lowest large (s >= T)
+// group, so the table is a pure function of the counts. Masks, ranks and
+// the total come from ballots and shuffles; the pairing loop runs at most
+// m - 1 times. Replaces the single-lane float construction of
+// include/Bingo.cuh:111-158.
+__device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uint32_t base, AliasRec* out) {
+  const unsigned long long mass = (unsigned long long)cnt << lane;
+  const uint32_t nz = __ballot_sync(kFull, cnt != 0);
+  const uint32_t m = __popc(nz);
+  if (m == 0) return 0;
+  const unsigned long long T = warp_sum_u64(mass);
+  unsigned __int128 s = (unsigned __int128)mass * m;
+  uint32_t small = __ballot_sync(kFull, cnt != 0 && s < T);
+  uint32_t large = nz & ~small;
+  unsigned long long thr = T;
+  int alias_lane = lane;
+  while (small && large) {
+    const int a = __ffs(small) - 1, b = __ffs(large) - 1;
+    const unsigned long long sa = __shfl_sync(kFull, (unsigned long long)s, a);  // s_a < T fits 64 bits
+    if (lane == a) {
+      thr = sa;
+      alias_lane = b;
+    }
+    if (lane == b) s -= (unsigned __int128)(T - sa);
+    small &= ~(1u << a);
+    const bool b_small = __shfl_sync(kFull, (int)(s < T), b);
+    if (b_small) {
+      large &= ~(1u << b);
+      small |= 1u << b;
+    }
+  }
+  // Remaining groups hold exactly T: thr = T, alias = self (already set).
+  const uint32_t alt_base = __shfl_sync(kFull, base, alias_lane);
+  const uint32_t alt_cnt = __shfl_sync(kFull, cnt, alias_lane);
+  if (cnt) {
+    const uint32_t j = __popc(nz & lanemask_lt());
+    AliasRec r;
+    r.thr = thr;
+    r.T = T;
+    r.own_base = base;
+    r.own_cnt = cnt;
+    r.alt_base = alt_base;
+    r.alt_cnt = alt_cnt;
+    out[j] = r;
+  }
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Adjacency index (node2vec neighbour test), linear probing on mix32.
+__device__ __forceinline__ void hash_add(HashEntry* tab, uint32_t hmask, uint32_t v, uint32_t* claimed) {
+  uint32_t h = mix32(v) & hmask;
+  for (uint32_t probe = 0; probe <= hmask; ++probe) {
+    const int prev = atomicCAS(&tab[h].key, kEmptyKey, (int)v);
+    if (prev == kEmptyKey || prev == (int)v) {
+      atomicAdd(&tab[h].cnt, 1);
+      if (prev == kEmptyKey) ++*claimed;
+      return;
+    }
+    h = (h + 1) & hmask;
+  }
+}
+
+__device__ __forceinline__ void hash_sub(HashEntry* tab, uint32_t hmask, uint32_t v) {
+  uint32_t h = mix32(v) & hmask;
+  for (uint32_t probe = 0; probe <= hmask; ++probe) {
+    const int k = tab[h].key;
+    if (k == (int)v) {
+      atomicSub(&tab[h].cnt, 1);
+      return;
+    }
+    if (k == kEmptyKey) return;
+    h = (h + 1) & hmask;
+  }
+}
+
+__device__ __forceinline__ bool hash_has(const HashEntry* tab, uint32_t hmask, uint32_t v) {
+  uint32_t h = mix32(v) & hmask;
+  for (uint32_t probe = 0; probe <= hmask; ++probe) {
+    const HashEntry e = tab[h];
+    if (e.key == (int)v) return e.cnt > 0;
+    if (e.key == kEmptyKey) return false;
+    h = (h + 1) & hmask;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Growth plan for appending `len` edges to a vertex. All lanes compute the
+// same values; lane k also knows whether group k grows and to what capacity.
+struct GrowPlan {
+  uint32_t new_ecap;   // 0 = no edge relocation
+  uint32_t new_bpcap;  // 0 = no back-pointer relocation
+  uint32_t new_acap;   // 0 = alias table fits
+  uint32_t new_hcap;   // 0 = adjacency index fits
+  uint32_t gcap_lane;  // this lane's new group capacity, 0 = fits
+  uint32_t gsum;       // sum over lanes of gcap_lane
+  uint32_t gpre;       // exclusive prefix of gcap_lane over lanes
+};
+
+// add_lane: how many of the appended edges carry bit `lane`; pc_total: sum of
+// their popcounts. Called with the whole warp.
+__device__ __forceinline__ GrowPlan plan_growth(int lane, const VertexMeta& M, const GroupDesc& G, uint32_t len,
+                                                uint32_t add_lane, uint32_t pc_total, uint32_t node2vec) {
+  GrowPlan p;
+  const uint32_t ecnt = M.ecnt + len;
+  p.new_ecap = ecnt > M.ecap ? pow2_at_least(ecnt, kMinEdgeCap) : 0;
+  const uint32_t bpn = M.bpcnt + pc_total;
+  p.new_bpcap = bpn > M.bpcap ? pow2_at_least(bpn, kMinEdgeCap) : 0;
+  const uint32_t cnt = G.cnt + add_lane;
+  p.gcap_lane = cnt > G.cap ? pow2_at_least(cnt, kMinGroupCap) : 0;
+  const uint32_t incl = warp_incl_scan(p.gcap_lane, lane);
+  p.gsum = __shfl_sync(kFull, incl, 31);
+  p.gpre = incl - p.gcap_lane;
+  const uint32_t m = __popc(__ballot_sync(kFull, cnt != 0));
+  p.new_acap = m > M.acap ? pow2_at_least(m, 1) : 0;
+  p.new_hcap = 0;
+  if (node2vec && (M.hkeys + len > M.hcap / 2)) p.new_hcap = pow2_at_least(2 * (M.live + len), kMinHashCap);
+  return p;
+}
+
+// Per-lane count of segment edges carrying bit `lane`, and the segment's
+// total popcount, from one ballot per bit per 32 edges.
+__device__ __forceinline__ void count_bits(int lane, const uint32_t* seg_w, uint32_t len, uint32_t* add_lane,
+                                           uint32_t* pc_total) {
+  uint32_t add = 0, pc = 0;
+  for (uint32_t c = 0; c < len; c += 32) {
+    const uint32_t i = c + lane;
+    const uint32_t w = i < len ? seg_w[i] : 0u;
+    pc += __popc(w);
+    uint32_t present = __reduce_or_sync(kFull, w);
+    while (present) {
+      const int k = __ffs(present) - 1;
+      present &= present - 1;
+      const uint32_t b = __ballot_sync(kFull, (w >> k) & 1u);
+      if (lane == k) add += __popc(b);
+    }
+  }
+  *add_lane = add;
+  *pc_total = warp_sum_u32(pc);
+}
+
+// Warp copy of n 32-bit words.
+__device__ __forceinline__ void warp_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n, int lane) {
+  for (uint32_t i = lane; i < n; i += 32) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// Apply a growth plan (relocations drawn from per-arena bases reserved for
+// this segment), append the segment's edges in order, refresh the adjacency
+// index and rebuild the alias table. Replaces NodeData::copy / insert /
+// buildAliasTable (include/Bingo.cuh:95-110, :182-198, :111-158) and the host
+// reMalloc round trip (include/operation.cuh:163-174).
+//
+// seg_v / seg_w / seg_orig: the segment's edges in batch order; out_slots is
+// indexed by seg_orig (may be null). res[a]: the arena offsets reserved for
+// this segment (units of each arena).
+static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32_t* seg_v, const uint32_t* seg_w,
+                             const uint32_t* seg_orig, uint32_t len, uint32_t* out_slots,
+                             const unsigned long long res[kArenas]) {
+  const int lane = threadIdx.x & 31;
+  VertexMeta M = S.meta[u];
+  GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
+  uint32_t add_lane, pc_total;
+  count_bits(lane, seg_w, len, &add_lane, &pc_total);
+  const GrowPlan P = plan_growth(lane, M, G, len, add_lane, pc_total, S.node2vec);
+
+  // --- relocations (old contents keep their order) ---
+  if (P.new_ecap) {
+    EdgeRec* dst = S.edges + res[A_EDGE];
+    const EdgeRec* src = S.edges + M.eoff;
+    for (uint32_t i = lane; i < M.ecnt; i += 32) dst[i] = src[i];
+    M.eoff = res[A_EDGE];
+    M.ecap = P.new_ecap;
+  }
+  if (P.new_bpcap) {
+    warp_copy_u32(S.bp + res[A_BP], S.bp + M.bpoff, M.bpcnt, lane);
+    M.bpoff = res[A_BP];
+    M.bpcap = P.new_bpcap;
+  }
+  {
+    uint32_t grow = __ballot_sync(kFull, P.gcap_lane != 0);
+    while (grow) {
+      const int k = __ffs(grow) - 1;
+      grow &= grow - 1;
+      const uint32_t ob = __shfl_sync(kFull, G.base, k), oc = __shfl_sync(kFull, G.cnt, k);
+      const unsigned long long nb = res[A_MEMBER] + __shfl_sync(kFull, P.gpre, k);  // entries
+      warp_copy_u32(S.gv + nb, S.gv + (size_t)ob * 4, oc, lane);
+      warp_copy_u32(S.gs + nb, S.gs + (size_t)ob * 4, oc, lane);
+      if (lane == k) {
+        G.base = (uint32_t)(nb >> 2);
+        G.cap = P.gcap_lane;
+      }
+    }
+  }
+  VertexRec R = S.vrec[u];
+  if (P.new_acap) {
+    R.aoff = (uint32_t)res[A_ALIAS];
+    M.acap = P.new_acap;
+  }
+  __syncwarp();
+
+  // --- append in batch order ---
+  uint32_t bpbase = M.bpcnt;
+  for (uint32_t c = 0; c < len; c += 32) {
+    const uint32_t i = c + lane;
+    const bool valid = i < len;
+    const uint32_t v = valid ? seg_v[i] : 0u, w = valid ? seg_w[i] : 0u;
+    const uint32_t pc = __popc(w);
+    const uint32_t incl = warp_incl_scan(pc, lane);
+    const uint32_t ebp = bpbase + incl - pc;
+    bpbase += __shfl_sync(kFull, incl, 31);
+    const uint32_t slot = M.ecnt + i;
+    if (valid) {
+      S.edges[M.eoff + slot] = EdgeRec{v, w, ebp, 0u};
+      if (out_slots) out_slots[seg_orig[i]] = slot;
+    }
+    uint32_t present = __reduce_or_sync(kFull, w);
+    while (present) {
+      const int k = __ffs(present) - 1;
+      present &= present - 1;
+      const bool has = (w >> k) & 1u;
+      const uint32_t b = __ballot_sync(kFull, has);
+      const uint32_t kcnt = __shfl_sync(kFull, G.cnt, k), kbase = __shfl_sync(kFull, G.base, k);
+      if (has) {
+        const uint32_t pos = kcnt + __popc(b & lanemask_lt());
+        const size_t e = (size_t)kbase * 4 + pos;
+        S.gv[e] = v;
+        S.gs[e] = slot;
+        S.bp[M.bpoff + ebp + __popc(w & ((1u << k) - 1u))] = pos;
+      }
+      if (lane == k) G.cnt += __popc(b);
+    }
+  }
+  M.ecnt += len;
+  M.bpcnt = bpbase;
+  M.live += len;
+  __syncwarp();
+
+  // --- adjacency index ---
+  if (S.node2vec) {
+    uint32_t claimed = 0;
+    if (P.new_hcap) {
+      // Rebuild from every live slot into a fresh table.
+      HashEntry* tab = S.hash + res[A_HASH];
+      for (uint32_t i = lane; i < P.new_hcap; i += 32) tab[i] = HashEntry{kEmptyKey, 0};
+      __syncwarp();
+      for (uint32_t i = lane; i < M.ecnt; i += 32) {
+        const EdgeRec e = S.edges[M.eoff + i];
+        if (e.w) hash_add(tab, P.new_hcap - 1, e.v, &claimed);
+      }
+      R.hoff = (uint32_t)res[A_HASH];
+      R.hmask = P.new_hcap - 1;
+      M.hcap = P.new_hcap;
+      M.hkeys = warp_sum_u32(claimed);
+    } else {
+      for (uint32_t i = lane; i < len; i += 32) hash_add(S.hash + R.hoff, R.hmask, seg_v[i], &claimed);
+      M.hkeys += warp_sum_u32(claimed);
+    }
+  }
+  __syncwarp();
+
+  // --- alias table over the new counts ---
+  R.m = warp_build_alias(lane, G.cnt, G.base, S.alias + R.aoff);
+  S.gdesc[(size_t)u * kBits + lane] = G;
+  if (lane == 0) {
+    S.meta[u] = M;
+    S.vrec[u] = R;
+  }
+}
+
+// Per-arena sizes the append of a segment needs (same decisions as
+// apply_append). Lane 0 returns them.
+__device__ __forceinline__ void plan_append(const StoreView& S, uint32_t u, const uint32_t* seg_w, uint32_t len,
+                                            unsigned long long need[kArenas]) {
+  const int lane = threadIdx.x & 31;
+  const VertexMeta M = S.meta[u];
+  const GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
+  uint32_t add_lane, pc_total;
+  count_bits(lane, seg_w, len, &add_lane, &pc_total);
+  const GrowPlan P = plan_growth(lane, M, G, len, add_lane, pc_total, S.node2vec);
+  need[A_MEMBER] = P.gsum;
+  need[A_EDGE] = P.new_ecap;
+  need[A_BP] = P.new_bpcap;
+  need[A_ALIAS] = P.new_acap;
+  need[A_HASH] = P.new_hcap;
+}
+
+// ---------------------------------------------------------------------------
+// Delete a run of slots of one vertex in order: swap-remove the slot from
+// each of its groups (lane k = group k), tombstone it, then rebuild the alias
+// table. Replaces NodeData::deleteE (include/Bingo.cuh:199-218) and the
+// tombstone loop of deleteKernel (include/operation.cuh:209-210).
+static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32_t* seg_slot, uint32_t len) {
+  const int lane = threadIdx.x & 31;
+  VertexMeta M = S.meta[u];
+  GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
+  VertexRec R = S.vrec[u];
+  uint32_t rejected = 0;
+  for (uint32_t d = 0; d < len; ++d) {
+    const uint32_t slot = seg_slot[d];
+    EdgeRec e{0, 0, 0, 0};
+    if (slot < M.ecnt) e = S.edges[M.eoff + slot];
+    if (e.w == 0) {
+      ++rejected;
+      continue;
+    }
+    if ((e.w >> lane) & 1u) {
+      const size_t gb = (size_t)G.base * 4;
+      const uint32_t pos = S.bp[M.bpoff + e.ebp + __popc(e.w & lanemask_lt())];
+      const uint32_t last = G.cnt - 1;
+      const uint32_t ms = S.gs[gb + last];
+      S.gv[gb + pos] = S.gv[gb + last];
+      S.gs[gb + pos] = ms;
+      const EdgeRec em = S.edges[M.eoff + ms];
+      S.bp[M.bpoff + em.ebp + __popc(em.w & lanemask_lt())] = pos;
+      G.cnt = last;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      S.edges[M.eoff + slot].w = 0u;
+      if (S.node2vec && R.hmask) hash_sub(S.hash + R.hoff, R.hmask, e.v);
+    }
+    --M.live;
+    __syncwarp();
+  }
+  if (rejected && lane == 0) {
+    atomicAdd(&S.err[1], rejected);
+    set_err(S.err, E_INVALID_SLOT);
+  }
+  R.m = warp_build_alias(lane, G.cnt, G.base, S.alias + R.aoff);
+  S.gdesc[(size_t)u * kBits + lane] = G;
+  if (lane == 0) {
+    S.meta[u] = M;
+    S.vrec[u] = R;
+  }
+}
+
+}  // namespace bingo

@@ -1,0 +1,224 @@
+"""Host-side interface of the B200 walk engine.
+
+`Graph` mirrors the reference's operator surface (include/operation.cuh:
+``build`` :33, ``insert`` :144, ``deleteE`` :215 and the walk kernels
+:252-430 launched by ``randomWalk``, include/graph.cuh:93) over the C ABI in
+include/bingo.h. Arrays may be numpy arrays (host) or CUDA tensors (device);
+ids are 0-based. Errors raise `BingoError` carrying the C status.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from ._lib import BingoConfig, BingoError, BingoStats, BingoWalkJob, lib
+
+DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
+APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
+WALK_PPR_TAIL = 1
+BATCHED, PLAIN = 0, 1
+
+
+def _u32(a):
+    """Pointer + keep-alive for a uint32 array (numpy host array or CUDA tensor)."""
+    if a is None:
+        return None, None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        if a.element_size() != 4:
+            raise ValueError("expected a 32-bit tensor")
+        return ctypes.c_void_p(a.data_ptr()), a
+    arr = np.ascontiguousarray(a, dtype=np.uint32)
+    return ctypes.c_void_p(arr.ctypes.data), arr
+
+
+def _out(a, dtype):
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr()), a
+    if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous):
+        raise ValueError(f"output must be a contiguous numpy {np.dtype(dtype)} array or a tensor")
+    return ctypes.c_void_p(a.ctypes.data), a
+
+
+@dataclass
+class WalkJob:
+    """One walk job (bingo_walk_job). starts=None walks [first, first+n_starts)."""
+    app: int = DEEPWALK
+    length: int = 80
+    starts: Optional[object] = None
+    n_starts: int = 0
+    first: int = 0
+    job_id: int = 0
+    seed: int = 0
+    flags: int = 0
+    p: float = 0.5
+    q: float = 2.0
+    stop_prob: float = 0.0125
+    out: Optional[object] = None
+
+
+class Graph:
+    """A dynamic weighted graph resident on one GPU."""
+
+    def __init__(self, device: int = 0, node2vec: bool = True, synchronous: bool = True,
+                 arena_factor: float = 2.0, arena_bytes: int = 0):
+        L = lib()
+        cfg = BingoConfig()
+        L.bingo_config_init(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.node2vec = 1 if node2vec else 0
+        cfg.synchronous = 1 if synchronous else 0
+        cfg.arena_factor = arena_factor
+        cfg.arena_bytes = arena_bytes
+        h = ctypes.c_void_p()
+        st = L.bingo_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st:
+            raise BingoError(st, (L.bingo_last_error(None) or b"").decode())
+        self._h = h
+        self._L = L
+        self.n = 0
+
+    # ------------------------------------------------------------------ util
+    def _check(self, st: int):
+        if st:
+            raise BingoError(st, (self._L.bingo_last_error(self._h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bingo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------------ ops
+    def load_edges(self, src, dst, w, n: int):
+        """Load a graph (reference build(), include/operation.cuh:33)."""
+        ps, ks = _u32(src)
+        pd, kd = _u32(dst)
+        pw, kw = _u32(w)
+        m = len(src) if not hasattr(src, "numel") else src.numel()
+        self._check(self._L.bingo_load_edges(self._h, ps, pd, pw, m, n))
+        self.n = n
+
+    def insert_batch(self, src, dst, w, out_slots=None, return_slots: bool = True):
+        """Append a batch of edges (reference insert(), include/operation.cuh:144).
+        Returns the slot id of every edge (numpy) unless out_slots is given."""
+        k = len(src) if not hasattr(src, "numel") else src.numel()
+        ps, ks = _u32(src)
+        pd, kd = _u32(dst)
+        pw, kw = _u32(w)
+        if out_slots is None and return_slots:
+            out_slots = np.empty(k, dtype=np.uint32)
+        po, ko = _out(out_slots, np.uint32) if out_slots is not None else (None, None)
+        self._check(self._L.bingo_insert_batch(self._h, ps, pd, pw, k, po))
+        return out_slots
+
+    def delete_batch(self, u, slot):
+        """Delete (vertex, slot) pairs (reference deleteE(), include/operation.cuh:215)."""
+        k = len(u) if not hasattr(u, "numel") else u.numel()
+        pu, ku = _u32(u)
+        psl, ksl = _u32(slot)
+        self._check(self._L.bingo_delete_batch(self._h, pu, psl, k))
+
+    def walk_jobs(self, jobs: Sequence[WalkJob], mode: int = BATCHED):
+        """Run a list of walk jobs; each job's out must be preallocated."""
+        arr = (BingoWalkJob * len(jobs))()
+        keep = []
+        for i, j in enumerate(jobs):
+            ps, ks = _u32(j.starts) if j.starts is not None else (None, None)
+            po, ko = _out(j.out, np.int32)
+            keep += [ks, ko]
+            arr[i].app = j.app
+            arr[i].length = j.length
+            arr[i].starts = ps
+            arr[i].n_starts = j.n_starts
+            arr[i].first = j.first
+            arr[i].job_id = j.job_id
+            arr[i].seed = j.seed
+            arr[i].flags = j.flags
+            arr[i].p = j.p
+            arr[i].q = j.q
+            arr[i].stop_prob = j.stop_prob
+            arr[i].out = po
+        self._check(self._L.bingo_walk(self._h, arr, len(jobs), mode))
+
+    def walk(self, app: int = DEEPWALK, length: int = 80, starts=None, n_starts: Optional[int] = None,
+             first: int = 0, seed: int = 0, job_id: int = 0, p: float = 0.5, q: float = 2.0,
+             stop_prob: float = 0.0125, flags: int = 0, mode: int = PLAIN, out=None):
+        """One walk job; returns [n_starts][length] int32 (sampling: [n_starts])."""
+        if starts is not None:
+            n_starts = len(starts) if not hasattr(starts, "numel") else starts.numel()
+        if n_starts is None:
+            n_starts = self.n - first
+        if out is None:
+            out = np.empty((n_starts,) if app == SAMPLING else (n_starts, length), dtype=np.int32)
+        self.walk_jobs([WalkJob(app=app, length=length, starts=starts, n_starts=n_starts, first=first,
+                                job_id=job_id, seed=seed, flags=flags, p=p, q=q, stop_prob=stop_prob,
+                                out=out)], mode=mode)
+        return out
+
+    def sync(self):
+        self._check(self._L.bingo_sync(self._h))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._L.bingo_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def stats(self) -> dict:
+        s = BingoStats()
+        self._check(self._L.bingo_get_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in BingoStats._fields_ if f != "reserved0"}
+
+    def dump(self) -> dict:
+        """Full graph state in the layout the CPU oracle dumps (numpy arrays)."""
+        sizes = (ctypes.c_uint64 * 3)()
+        self._check(self._L.bingo_dump_sizes(self._h, sizes))
+        ns, nm, na = sizes[0], sizes[1], sizes[2]
+        n = self.n
+        d = dict(
+            ecnt=np.zeros(n, np.uint32), live=np.zeros(n, np.uint32), ev=np.zeros(ns, np.uint32),
+            ew=np.zeros(ns, np.uint32), gcnt=np.zeros(n * 32, np.uint32), mslot=np.zeros(nm, np.uint32),
+            mv=np.zeros(nm, np.uint32), mbp=np.zeros(nm, np.uint32), am=np.zeros(n, np.uint32),
+            athr=np.zeros(na, np.uint64), aT=np.zeros(na, np.uint64), aown=np.zeros(na, np.uint8),
+            aalias=np.zeros(na, np.uint8))
+        order = ["ecnt", "live", "ev", "ew", "gcnt", "mslot", "mv", "mbp", "am", "athr", "aT", "aown", "aalias"]
+        ptrs = [ctypes.c_void_p(d[k].ctypes.data) for k in order]
+        self._check(self._L.bingo_dump_state(self._h, *ptrs))
+        return d
+
+    def philox(self, ctr: np.ndarray, key: int) -> np.ndarray:
+        ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
+        out = np.zeros_like(ctr)
+        self._check(self._L.bingo_philox(self._h, ctypes.c_void_p(ctr.ctypes.data), ctr.shape[0], key,
+                                         ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+    # ---------------------------------------------- reference-named aliases
+    def build(self, src, dst, w, n: int):
+        """Alias of load_edges under the reference's name (include/operation.cuh:33)."""
+        return self.load_edges(src, dst, w, n)
+
+    def insert(self, src, dst, w):
+        """Alias of insert_batch under the reference's name (include/operation.cuh:144)."""
+        return self.insert_batch(src, dst, w)
+
+    def deleteE(self, u, slot):
+        """Alias of delete_batch under the reference's name (include/operation.cuh:215)."""
+        return self.delete_batch(u, slot)

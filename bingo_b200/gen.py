@@ -1,0 +1,65 @@
+"""Seeded synthetic workloads (include/bingo_gen.h): R-MAT graphs, weight
+distributions and update batches. These stand in for the reference's dataset
+files (include/graph.cuh:22-27) and its update generators
+(include/graph.cuh:58-92), which need data that is not available."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import lib
+
+W_UNIFORM, W_LOGUNIFORM, W_ZIPF = 0, 1, 2
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1):
+    """R-MAT edges (src, dst) as uint32, sorted by (src, dst), no self-loops or duplicates."""
+    cap = edge_factor << scale
+    src = np.empty(cap, np.uint32)
+    dst = np.empty(cap, np.uint32)
+    m = lib().bingo_gen_rmat(scale, edge_factor, a, b, c, seed, _p(src), _p(dst))
+    return src[:m].copy(), dst[:m].copy()
+
+
+def weights(m: int, dist: int = W_UNIFORM, lo: float = 1, hi: float = 1024, s: float = 1.2, seed: int = 2):
+    w = np.empty(m, np.uint32)
+    lib().bingo_gen_weights(m, dist, lo, hi, s, seed, _p(w))
+    return w
+
+
+class UpdateGen:
+    """Absent-pair inserts and uniform live-edge deletes, tracking slots the
+    way the engine assigns them (append order per vertex)."""
+
+    def __init__(self, n: int, src: np.ndarray, dst: np.ndarray, seed: int = 3):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        self._L = lib()
+        self._g = self._L.bingo_updgen_create(n, _p(src), _p(dst), len(src), seed)
+
+    def inserts(self, k: int, dist: int = W_UNIFORM, lo: float = 1, hi: float = 1024, s: float = 1.2):
+        src = np.empty(k, np.uint32)
+        dst = np.empty(k, np.uint32)
+        w = np.empty(k, np.uint32)
+        self._L.bingo_updgen_inserts(self._g, k, dist, lo, hi, s, _p(src), _p(dst), _p(w))
+        return src, dst, w
+
+    def deletes(self, k: int):
+        u = np.empty(k, np.uint32)
+        slot = np.empty(k, np.uint32)
+        made = self._L.bingo_updgen_deletes(self._g, k, _p(u), _p(slot))
+        return u[:made].copy(), slot[:made].copy()
+
+    @property
+    def live(self) -> int:
+        return self._L.bingo_updgen_live(self._g)
+
+    def __del__(self):
+        if getattr(self, "_g", None):
+            self._L.bingo_updgen_destroy(self._g)
+            self._g = None

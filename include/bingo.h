@@ -1,0 +1,166 @@
+/*
+ * bingo.h - C ABI of the B200 radix bias-factorization walk engine.
+ *
+ * The reference has no library boundary: its operator surface is a set of
+ * C++ host functions and CUDA kernels called from its graph driver
+ * (include/graph.cuh). Each entry point below names the reference interface
+ * it replaces. Every function returns a bingo_status (0 = BINGO_OK); no C++
+ * exception crosses this boundary. Vertex ids are 0-based in [0, n).
+ *
+ * Pointers: every array argument may be host memory (pageable or pinned) or
+ * device memory on the handle's device; the library detects which. Calls are
+ * ordered on the handle's CUDA stream. With cfg.synchronous != 0 (the
+ * default) each call returns only after its device work is complete and
+ * reports device-detected errors directly; otherwise such errors surface at
+ * the next bingo_sync().
+ *
+ * Threading: one handle may be used by one host thread at a time.
+ */
+#ifndef BINGO_H
+#define BINGO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bingo_handle bingo_handle;
+
+typedef enum bingo_status {
+  BINGO_OK = 0,
+  BINGO_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad enum, bad config */
+  BINGO_ERR_OUT_OF_RANGE = 2,     /* a vertex id >= n */
+  BINGO_ERR_ZERO_WEIGHT = 3,      /* an inserted or loaded weight of 0 */
+  BINGO_ERR_INVALID_SLOT = 4,     /* delete of an absent or already deleted slot (skipped) */
+  BINGO_ERR_CAPACITY = 5,         /* the graph arena (HBM budget) cannot hold the batch */
+  BINGO_ERR_CUDA = 6,             /* a CUDA runtime call failed; see bingo_last_error */
+  BINGO_ERR_NOT_LOADED = 7,       /* operation needs a loaded graph */
+  BINGO_ERR_TIMEOUT = 8,          /* a bounded device wait expired */
+  BINGO_ERR_NO_DEVICE = 9,        /* no usable CUDA device */
+  BINGO_ERR_UNSUPPORTED = 10      /* e.g. node2vec without the adjacency index */
+} bingo_status;
+
+typedef enum bingo_app {
+  BINGO_DEEPWALK = 0, /* include/operation.cuh:252 deepwalkKernel */
+  BINGO_NODE2VEC = 1, /* include/operation.cuh:281 node2vecKernel */
+  BINGO_PPR = 2,      /* include/operation.cuh:336 pprKernel */
+  BINGO_SAMPLING = 3  /* include/operation.cuh:407 samplingKernel (one hop) */
+} bingo_app;
+
+/* bingo_walk_job.flags */
+#define BINGO_WALK_PPR_TAIL 1u /* PPR keeps walking past the last slot and overwrites it,
+                                  as include/operation.cuh:353-360 does */
+
+/* bingo_walk() mode */
+#define BINGO_WALK_BATCHED 0u /* all jobs in one persistent launch over a device work queue */
+#define BINGO_WALK_PLAIN 1u   /* one launch per job, the reference's per-job form */
+
+typedef struct bingo_config {
+  int32_t device;         /* CUDA device ordinal */
+  uint32_t node2vec;      /* maintain the adjacency index node2vec needs (like NODE2VEC, include/api.h:25) */
+  uint32_t synchronous;   /* 1: every call waits for its device work (default) */
+  uint32_t reserved0;
+  double arena_factor;    /* graph arena = factor x bytes needed at load (default 2.0) */
+  uint64_t arena_bytes;   /* minimum graph arena bytes; 0 = from arena_factor only */
+} bingo_config;
+
+typedef struct bingo_walk_job {
+  int32_t app;            /* bingo_app */
+  uint32_t length;        /* positions per walk, start included (reference LEN=80) */
+  const uint32_t* starts; /* start vertices; NULL = the range [first, first + n_starts) */
+  uint64_t n_starts;
+  uint32_t first;
+  uint32_t job_id;        /* Philox counter word 3 */
+  uint64_t seed;          /* Philox key */
+  uint32_t flags;         /* BINGO_WALK_* */
+  uint32_t reserved0;
+  double p, q;            /* node2vec return / in-out parameters (reference P=0.5, Q=2) */
+  double stop_prob;       /* PPR termination probability (reference TP=0.0125) */
+  int32_t* out;           /* [n_starts][length] vertex ids, -1 after a dead end or stop;
+                             sampling: [n_starts] */
+} bingo_walk_job;
+
+typedef struct bingo_stats {
+  uint32_t n;             /* vertices */
+  uint32_t reserved0;
+  uint64_t slots;         /* edge slots including tombstones */
+  uint64_t live_edges;
+  uint64_t arena_bytes;   /* bytes reserved for the graph arenas */
+  uint64_t arena_used;    /* bytes handed out (live + abandoned by growth) */
+  uint64_t scratch_bytes; /* staging and sort scratch currently held */
+  uint64_t walk_steps;    /* walk steps produced since bingo_create (moves to a neighbour) */
+  uint64_t kernel_launches; /* engine kernels launched since bingo_create (library sort/scan/select
+                               kernels not included) */
+} bingo_stats;
+
+/* Defaults for bingo_config (device 0, node2vec on, synchronous, factor 2). */
+void bingo_config_init(bingo_config* cfg);
+
+/* Replaces the global device state of include/graph.cuh:9-14 and MemPool::init
+ * (include/gpuMem.cuh:15-24). */
+int bingo_create(const bingo_config* cfg, bingo_handle** out);
+int bingo_destroy(bingo_handle* h);
+
+/* Message of the last failing call on this handle (or of bingo_create when h is NULL). */
+const char* bingo_last_error(const bingo_handle* h);
+
+/* Replaces build(Edges*, int amount, NodeData**, NodeData**, int* d, int** sizeManager, int n)
+ * (include/operation.cuh:33). Edges of one source keep their input order as
+ * slots 0..deg-1 (the stable bucket of include/operation.cuh:82-90). */
+int bingo_load_edges(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m,
+                     uint32_t n);
+
+/* Replaces insert(Edges*, int amount, NodeData**, NodeData**, int* d, int* sizeManager)
+ * (include/operation.cuh:144). Edges append to their source in batch order
+ * (the stable_sort of include/operation.cuh:147). out_slots (may be NULL)
+ * receives each edge's slot id, the id the reference caller tracks as d[u]++
+ * (include/graph.cuh:66) and later passes to delete. Weight 0 is rejected. */
+int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k,
+                       uint32_t* out_slots);
+
+/* Replaces deleteE(Deleted*, int amount, NodeData**) (include/operation.cuh:215)
+ * with (u, slot) pairs (include/type.h:32-35). Deletes of one vertex apply in
+ * batch order; a slot that is absent or already deleted is skipped and the
+ * call returns BINGO_ERR_INVALID_SLOT after applying the rest. */
+int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot, uint64_t k);
+
+/* Replaces the walk kernels deepwalkKernel / node2vecKernel / pprKernel /
+ * samplingKernel<<<BLKSZ, THDSZ>>>(gId, pId, n, NodeData*, int* rwD, PIECESIZE, seed)
+ * (include/operation.cuh:252, :281, :336, :407) and the randomWalk driver
+ * (include/graph.cuh:93). Output rows match rwD ([walk][length]). mode is
+ * BINGO_WALK_BATCHED or BINGO_WALK_PLAIN; both give identical results. */
+int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
+
+/* Waits for all queued work; returns the first device-detected error since
+ * the previous bingo_sync (or BINGO_OK). */
+int bingo_sync(bingo_handle* h);
+
+/* The CUDA stream calls are ordered on (cudaStream_t as void*); NULL restores
+ * the handle's own stream. */
+int bingo_set_stream(bingo_handle* h, void* stream);
+
+int bingo_get_stats(bingo_handle* h, bingo_stats* out);
+
+/* Graph-state dump for parity checks (the reference has none; its state is
+ * the NodeData records of include/Bingo.cuh:6-58). sizes[0] = slots,
+ * sizes[1] = group members, sizes[2] = alias slots. All outputs are host
+ * arrays: ecnt/live/am [n]; ev/ew [slots] by vertex; gcnt [n*32];
+ * mslot/mv/mbp [members] by (vertex, bit): member slot, neighbour, and the
+ * slot's back-pointer (equals the member's position); athr/aT/aown/aalias
+ * [alias slots] by vertex: threshold, total mass, own bit, alias bit. */
+int bingo_dump_sizes(bingo_handle* h, uint64_t sizes[3]);
+int bingo_dump_state(bingo_handle* h, uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, uint32_t* gcnt,
+                     uint32_t* mslot, uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT,
+                     uint8_t* aown, uint8_t* aalias);
+
+/* Philox4x32-10 as the device computes it (one block per counter), for
+ * checking the walk random stream: out[4*i..4*i+3] = philox(ctr_i, key). */
+int bingo_philox(bingo_handle* h, const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BINGO_H */
