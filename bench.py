@@ -84,7 +84,7 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -221,7 +221,9 @@ def run_ours(args):
 
     total = args.warmup + args.steps
     n, src, dst, w, batches = make_workload(total)
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated (non-default) stream shared by torch's events and the engine.
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     g = Graph(device=local, synchronous=False)
     g.set_stream(stream.cuda_stream)
     g.load_edges(src, dst, w, n)
@@ -247,15 +249,15 @@ def run_ours(args):
                              out=out)], mode=PLAIN)
         ev["w1"][i].record(stream)
 
+    clocks = Clocks(local)
+    clocks.start()  # samples through warm-up and the timed region
     for i in range(args.warmup):
         step(i)
     g.sync()
     torch.cuda.synchronize(dev)
     st0 = g.stats()
-    clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize(dev)
-    clocks.start()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)

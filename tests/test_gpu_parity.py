@@ -248,3 +248,28 @@ def test_multi_edges_and_reload():
     ex2 = po.ExactGraph(4)
     ex2.load(src[:2], dst[:2], w[:2])
     assert_exact_equal(g.dump(), ex2.dump())
+
+
+@pytest.mark.parametrize("path", sorted(__import__("glob").glob(
+    __import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "ref_*.npz"))))
+def test_cuda_state_matches_reference_binary(path):
+    """The CUDA path against the reference's own CUDA build: after the load
+    and after every batch, every list the reference keeps (sparse groups in
+    member order, back-pointers), the float masses below its load-time bit
+    length, slots, weights and tombstones equal the reference's dump."""
+    import json
+    from tests.helpers import compare_exact_vs_ref
+    z = np.load(path, allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    n = meta["n"]
+    g = Graph()
+    g.load_edges(z["src"], z["dst"], z["w"], n)
+    names = ["logt", "bits", "sz", "ecnt", "asz", "ev", "ew", "grouptp", "num", "gsz", "members", "midx", "ap",
+             "aa", "ab"]
+    for i, op in enumerate(["load"] + meta["ops"]):
+        if op == "ins":
+            g.insert_batch(z[f"op{i}_a"], z[f"op{i}_b"], z[f"op{i}_c"])
+        elif op == "del":
+            g.delete_batch(z[f"op{i}_a"], z[f"op{i}_b"])
+        ref = {k: z[f"dump{i}_{k}"] for k in names}
+        compare_exact_vs_ref(g.dump(), ref, n, check_alias_tol=5e-3)
