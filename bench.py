@@ -71,7 +71,7 @@ def traffic_per_step():
 
 class Clocks:
     """nvidia-smi sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
@@ -89,12 +89,14 @@ class Clocks:
         except (OSError, FileNotFoundError):
             self.proc = None
 
-    def stop(self):
+    def stop(self, t0: float, t1: float):
+        """Samples whose timestamp lies in the host-time window [t0, t1]."""
         if not self.proc:
             return None
         self.proc.terminate()
         self.proc.wait(timeout=10)
         self.f.close()
+        import datetime
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
@@ -102,6 +104,9 @@ class Clocks:
             if len(parts) < 9:
                 continue
             try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if not (t0 - 0.05 <= ts <= t1 + 0.05):
+                    continue
                 sm.append(float(parts[1]))
                 mx = max(mx, float(parts[2]))
             except ValueError:
@@ -149,27 +154,58 @@ def barrier(world: int):
 
 
 # --------------------------------------------------------------------------- CPU leg
-def cpu_sample(n, src, dst, w, batch, walks: int, seed: int):
-    """Time the oracle (OpenMP, all host threads) on one full update batch and
-    `walks` DeepWalk walks; extrapolate to a full step (n walks)."""
-    from oracle import pyoracle as po
-    ex = po.ExactGraph(n)
-    ex.load(src, dst, w)
-    (ins, dels) = batch
-    t0 = time.perf_counter()
-    ex.insert(*ins)
-    ex.delete(*dels)
-    t_upd = time.perf_counter() - t0
-    rng = np.random.default_rng(seed)
-    starts = np.sort(rng.choice(n, size=walks, replace=False)).astype(np.uint32)
-    t0 = time.perf_counter()
-    rows = ex.walk(0, WALK_LEN, starts, seed=seed, job_id=0)
-    t_walk = time.perf_counter() - t0
-    steps = int((rows >= 0).sum() - len(starts))
-    scale = n / walks
-    value = steps * scale / (t_upd + t_walk * scale)
-    return dict(value=value, t_update=t_upd, t_walk=t_walk, walk_steps=steps, walks=walks,
-                walk_steps_per_s=steps / t_walk, edge_updates_per_s=(len(ins[0]) + len(dels[0])) / t_upd)
+class CpuRun:
+    """The CPU oracle (OpenMP, all host threads) on the same graph: load once,
+    then per step one full update batch and a bounded walk sample."""
+
+    def __init__(self, n, src, dst, w):
+        from oracle import pyoracle as po
+        self.n = n
+        self.ex = po.ExactGraph(n)
+        self.ex.load(src, dst, w)
+
+    def step(self, batch, walks: int, seed: int):
+        ins, dels = batch
+        t0 = time.perf_counter()
+        self.ex.insert(*ins)
+        self.ex.delete(*dels)
+        t_upd = time.perf_counter() - t0
+        rng = np.random.default_rng(seed)
+        starts = np.sort(rng.choice(self.n, size=walks, replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        rows = self.ex.walk(0, WALK_LEN, starts, seed=seed, job_id=0)
+        t_walk = time.perf_counter() - t0
+        steps = int((rows >= 0).sum() - len(starts))
+        scale = self.n / walks  # extrapolate the walk sample to one walk per vertex
+        value = steps * scale / (t_upd + t_walk * scale)
+        return dict(value=value, t_update=t_upd, t_walk=t_walk, walk_steps=steps, walks=walks,
+                    walk_steps_per_s=steps / t_walk, edge_updates_per_s=(len(ins[0]) + len(dels[0])) / t_upd)
+
+
+def gather_ceiling(dev, gib: float = 4.0, reps: int = 5):
+    """Random-sector read ceiling of this GPU: a torch gather of 4-byte words
+    at uniformly random indices over a table larger than L2. Each index costs
+    one random 32-byte DRAM sector (plus 12 sequential bytes of index and
+    output). Returns sector GB/s (32 B per random read) and reads/s."""
+    import torch
+    n = int(gib * (1 << 30)) // 4
+    table = torch.zeros(n, dtype=torch.int32, device=dev)
+    k = 1 << 27
+    idx = torch.randint(0, n, (k,), device=dev, dtype=torch.int64)
+    out = torch.empty(k, dtype=torch.int32, device=dev)
+    torch.index_select(table, 0, idx, out=out)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e9
+    for _ in range(reps):
+        e0.record()
+        torch.index_select(table, 0, idx, out=out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del table, idx, out
+    return {"random_sector_gbs": k * 32 / best / 1e9, "random_reads_per_s": k / best,
+            "total_gbs": k * (32 + 12) / best / 1e9, "table_gib": gib}
 
 
 def run_reference(args):
@@ -183,8 +219,9 @@ def run_reference(args):
     n, src, dst, w, batches = make_workload(args.warmup + args.steps)
     walks = args.ref_walks
     vals, last = [], None
+    cpu = CpuRun(n, src, dst, w)
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(n, src, dst, w, batches[i], walks, seed=100 + i)
+        r = cpu.step(batches[i], walks, seed=100 + i)
         if i >= args.warmup:
             vals.append(r["value"])
             last = r
@@ -206,6 +243,55 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- GPU arm
+def run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world):
+    """The same steps through the C ABI with pinned host buffers: every step
+    copies its update batch in and its slot ids and walk rows out."""
+    import torch
+    from bingo_b200 import DEEPWALK, PLAIN, WalkJob
+    total = args.warmup + args.steps
+    g.load_edges(src, dst, w, n)
+    g.sync()
+
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory()
+        return t
+
+    hbatches = [((pinned(i[0]), pinned(i[1]), pinned(i[2])), (pinned(d[0]), pinned(d[1]))) for i, d in batches]
+    hout = torch.empty((n, WALK_LEN), dtype=torch.int32).pin_memory()
+    hslots = torch.empty(BATCH_INS, dtype=torch.int32).pin_memory()
+
+    def e2e_step(i):
+        (a, b, c), (du, ds) = hbatches[i]
+        g.insert_batch(a, b, c, out_slots=hslots)
+        g.delete_batch(du, ds)
+        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, starts=None, n_starts=n, first=0, job_id=i, seed=seed,
+                             out=hout)], mode=PLAIN)
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    g.sync()
+    torch.cuda.synchronize(dev)
+    st2 = g.stats()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.warmup, total):
+        e2e_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    g.sync()
+    st3 = g.stats()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), world, dev)
+    e2e_steps = reduce_sum(st3["walk_steps"] - st2["walk_steps"], world, dev)
+    h2d = BATCH_INS * 12 + BATCH_DEL * 8
+    d2h = n * WALK_LEN * 4 + BATCH_INS * 4
+
+    return {"value": e2e_steps / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h}
+
+
 def run_ours(args):
     import torch
 
@@ -250,7 +336,9 @@ def run_ours(args):
         ev["w1"][i].record(stream)
 
     clocks = Clocks(local)
-    clocks.start()  # samples through warm-up and the timed region
+    clocks.start()  # samples from the warm-up to the end of the e2e timed region
+    time.sleep(0.5)
+    t_busy0 = time.time()
     for i in range(args.warmup):
         step(i)
     g.sync()
@@ -266,7 +354,6 @@ def run_ours(args):
     t_end.record(stream)
     torch.cuda.synchronize(dev)
     barrier(world)
-    clk = clocks.stop()
     g.sync()
     st1 = g.stats()
     ms = t_start.elapsed_time(t_end)
@@ -279,44 +366,10 @@ def run_ours(args):
     value = steps_all / (ms_max / 1e3)
 
     # ---- e2e: same work through the C ABI with pinned host buffers
-    g.load_edges(src, dst, w, n)
-    g.sync()
-
-    def pinned(a):
-        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory()
-        return t
-
-    hbatches = [((pinned(i[0]), pinned(i[1]), pinned(i[2])), (pinned(d[0]), pinned(d[1]))) for i, d in batches]
-    hout = torch.empty((n, WALK_LEN), dtype=torch.int32).pin_memory()
-    hslots = torch.empty(BATCH_INS, dtype=torch.int32).pin_memory()
-
-    def e2e_step(i):
-        (a, b, c), (du, ds) = hbatches[i]
-        g.insert_batch(a, b, c, out_slots=hslots)
-        g.delete_batch(du, ds)
-        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, starts=None, n_starts=n, first=0, job_id=i, seed=seed,
-                             out=hout)], mode=PLAIN)
-
-    for i in range(args.warmup):
-        e2e_step(i)
-    g.sync()
-    torch.cuda.synchronize(dev)
-    st2 = g.stats()
-    barrier(world)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.warmup, total):
-        e2e_step(i)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    g.sync()
-    st3 = g.stats()
-    e2e_ms = reduce_max(e0.elapsed_time(e1), world, dev)
-    e2e_steps = reduce_sum(st3["walk_steps"] - st2["walk_steps"], world, dev)
-    h2d = BATCH_INS * 12 + BATCH_DEL * 8
-    d2h = n * WALK_LEN * 4 + BATCH_INS * 4
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world)
+    clk = clocks.stop(t_busy0, time.time())
 
     # ---- roofline of the walk kernel
     peak, peak_src = peak_hbm()
@@ -326,9 +379,11 @@ def run_ours(args):
             "traffic": (tps * steps_local / args.steps) if tps else None, "peak_source": peak_src,
             "kernel": "k_walk_plain<DEEPWALK>", "bytes_per_step": BYTES_PER_STEP}
 
+    if args.gather_ceiling:
+        roof["random_sector_ceiling"] = gather_ceiling(dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_sample(n, src, dst, w, batches[args.warmup], args.cpu_walks, seed=7)
+        r = CpuRun(n, src, dst, w).step(batches[0], args.cpu_walks, seed=7)
         cpu = {"value": r["value"], "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"one full 50K+50K update batch + {args.cpu_walks} walks x {WALK_LEN} on the CPU oracle "
                          f"(OpenMP), walk time scaled to {n} walks",
@@ -344,11 +399,11 @@ def run_ours(args):
                        "weights": "loguniform[1,2^20)", "walks": n, "walk_len": WALK_LEN,
                        "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}, "form": "plain (one launch per job)",
                        "l2": "inputs larger than L2 (graph state and 320 MB walk output per step)",
+                       "clocks": "nvidia-smi samples from warm-up to the end of the e2e timed region",
                        "parallelism": f"replicas x{world}"},
             "walk_steps_per_s": steps_local / (walk_ms / 1e3),
             "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * args.steps / (upd_ms / 1e3),
-            "e2e": {"value": e2e_steps / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clk,
@@ -369,7 +424,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-walks", type=int, default=131072)
     ap.add_argument("--ref-walks", type=int, default=131072)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--gather-ceiling", action="store_true",
+                    help="also measure the GPU's random 32-byte-sector read ceiling")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint
 __global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, const uint32_t* ctl) {
+  __shared__ uint32_t stage[kBlock / 32][64];
   if (*ctl) return;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
   const uint32_t nS = *nseg;
@@ -161,51 +162,99 @@ __global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint
     seg_bounds(seg, nS, s, k, &b, &e);
     const uint32_t u = skey[b];
     if (u >= S.n) continue;
-    apply_delete(S, u, sslot + b, e - b);
+    apply_delete(S, u, sslot + b, e - b, stage[threadIdx.x / 32]);
+  }
+}
+
+// Persistent walk kernel with per-lane refill. Each warp owns a range of
+// walk items and hands them to idle lanes; when the range runs out it pulls
+// the next kWalkChunk items from one device counter (reset by the host before
+// launch). APP >= 0: every item belongs to the single job J. APP < 0: items
+// index the concatenated jobs (prefix = running walk counts) and each lane
+// follows its own job's app.
+constexpr uint32_t kWalkChunk = 32;
+static_assert(kBlock % 32 == 0, "whole warps");
+
+// Resident 256-thread blocks per SM each walk variant is compiled for
+// (register budget 65536 / (256 * blocks)): DeepWalk and sampling 32
+// registers, PPR 40, node2vec 48, the mixed-job kernel 64.
+constexpr int walk_min_blocks(int app) {
+  return app == APP_DEEPWALK || app == APP_SAMPLING ? 8 : app == APP_PPR ? 6 : app == APP_NODE2VEC ? 5 : 4;
+}
+
+__device__ __forceinline__ bool begin_any(const WalkView& W, const WalkJobDev& J, uint32_t i, LaneWalk& s,
+                                          RowStage& o, int32_t (*obuf)[8], uint32_t& mv) {
+  switch (J.app) {
+    case APP_DEEPWALK: return walk_begin<APP_DEEPWALK>(W, J, i, s, o, obuf, mv);
+    case APP_NODE2VEC: return walk_begin<APP_NODE2VEC>(W, J, i, s, o, obuf, mv);
+    case APP_PPR: return walk_begin<APP_PPR>(W, J, i, s, o, obuf, mv);
+    default: return walk_begin<APP_SAMPLING>(W, J, i, s, o, obuf, mv);
+  }
+}
+__device__ __forceinline__ bool advance_any(const WalkView& W, const WalkJobDev& J, LaneWalk& s, RowStage& o,
+                                            int32_t (*obuf)[8], uint32_t& mv) {
+  switch (J.app) {
+    case APP_DEEPWALK: return walk_advance<APP_DEEPWALK>(W, J, s, o, obuf, mv);
+    case APP_NODE2VEC: return walk_advance<APP_NODE2VEC>(W, J, s, o, obuf, mv);
+    default: return walk_advance<APP_PPR>(W, J, s, o, obuf, mv);
   }
 }
 
 template <int APP>
-__global__ void __launch_bounds__(kBlock) k_walk_plain(WalkView W, WalkJobDev J) {
-  unsigned long long steps = 0;
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  // Uniform trip count across the warp so the closing shuffle sees all lanes.
-  const unsigned long long first = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u);
-  for (unsigned long long b = first; b < J.n; b += stride) {
-    const unsigned long long i = b + (threadIdx.x & 31);
-    if (i < J.n) steps += run_walk<APP>(W, J, (uint32_t)i);
-  }
-  add_steps(W, steps);
-}
-
-// Persistent walk kernel over a heterogeneous job list: warps pull 32 walks
-// at a time from one device counter (reset by the host before launch);
-// each lane decodes its own job by binary search over the walk prefix.
-__global__ void __launch_bounds__(kBlock) k_walk_batched(WalkView W, const WalkJobDev* jobs,
-                                                         const unsigned long long* prefix, uint32_t n_jobs,
-                                                         unsigned long long total, unsigned long long* queue) {
+__global__ void __launch_bounds__(kBlock, walk_min_blocks(APP)) k_walk(WalkView W, WalkJobDev J0, const WalkJobDev* __restrict__ jobs,
+                                                 const uint32_t* __restrict__ prefix, uint32_t n_jobs, uint32_t total,
+                                                 uint32_t* queue) {
+  __shared__ __align__(16) int32_t obuf[kBlock][8];
   const int lane = threadIdx.x & 31;
-  unsigned long long steps = 0;
+  LaneWalk s;
+  RowStage o{kNoSec, 0};
+  uint32_t jid = 0, moves = 0, wb = 0, we = 0;
+  bool active = false, drained = false;
   for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(queue, 32ull);
-    base = __shfl_sync(kFull, base, 0);
-    if (base >= total) break;
-    const unsigned long long item = base + lane;
-    if (item < total) {
-      uint32_t lo = 0, hi = n_jobs;
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (prefix[mid] <= item)
-          lo = mid;
-        else
-          hi = mid;
+    uint32_t idle = __ballot_sync(kFull, !active);
+    while (idle && !drained) {
+      if (wb >= we) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(queue, kWalkChunk);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= total) {
+          drained = true;
+          break;
+        }
+        wb = base;
+        we = min(base + kWalkChunk, total);
       }
-      const WalkJobDev J = jobs[lo];
-      steps += run_walk_any(W, J, (uint32_t)(item - prefix[lo]));
+      const uint32_t take = min((uint32_t)__popc(idle), we - wb);
+      const uint32_t rank = __popc(idle & lanemask_lt());
+      if (!active && rank < take) {
+        const uint32_t item = wb + rank;
+        if (APP >= 0) {
+          active = walk_begin<APP>(W, J0, item, s, o, obuf, moves);
+        } else {
+          uint32_t lo = 0, hi = n_jobs;
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (prefix[mid] <= item)
+              lo = mid;
+            else
+              hi = mid;
+          }
+          jid = lo;
+          active = begin_any(W, jobs[lo], item - prefix[lo], s, o, obuf, moves);
+        }
+      }
+      wb += take;
+      idle = __ballot_sync(kFull, !active);
+    }
+    if (!__any_sync(kFull, active)) break;
+    if (active) {
+      if (APP >= 0)
+        active = walk_advance<APP == APP_SAMPLING ? APP_DEEPWALK : APP>(W, J0, s, o, obuf, moves);
+      else
+        active = advance_any(W, jobs[jid], s, o, obuf, moves);
     }
   }
-  add_steps(W, steps);
+  add_steps(W, moves);
 }
 
 __global__ void k_philox(const uint32_t* ctr, unsigned long long count, uint32_t k0, uint32_t k1, uint32_t* out) {
@@ -217,6 +266,20 @@ __global__ void k_philox(const uint32_t* ctr, unsigned long long count, uint32_t
     out[4 * i + 2] = r.z;
     out[4 * i + 3] = r.w;
   }
+}
+
+// Resident 256-thread blocks per SM of walk kernel k_walk<APP> (register-limited):
+// the persistent grid is exactly one full wave.
+template <int APP>
+unsigned walk_blocks_per_sm() {
+  static int b = 0;
+  if (!b) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<APP>, kBlock, 0) != cudaSuccess || b <= 0) {
+      cudaGetLastError();
+      b = 4;
+    }
+  }
+  return (unsigned)b;
 }
 
 uint64_t prob_threshold(double p) {
@@ -658,7 +721,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   if (!jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
   if (mode != BINGO_WALK_BATCHED && mode != BINGO_WALK_PLAIN) throw Error(BINGO_ERR_INVALID_ARGUMENT, "bad mode");
   std::vector<WalkJobDev> dj(n_jobs);
-  std::vector<unsigned long long> prefix(n_jobs + 1, 0);
+  std::vector<uint64_t> prefix(n_jobs + 1, 0);
   // staging layout for host starts / outputs
   std::vector<uint64_t> s_off(n_jobs, ~0ull), o_off(n_jobs, ~0ull);
   uint64_t s_total = 0, o_total = 0;
@@ -686,7 +749,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     const uint64_t per = J.app == BINGO_SAMPLING ? 1 : J.length;
     if (J.n_starts && !is_device_ptr(J.out)) {
       o_off[j] = o_total;
-      o_total += J.n_starts * per;
+      o_total += (J.n_starts * per + 7) & ~7ull;  // 32-byte aligned job outputs
     }
     prefix[j + 1] = prefix[j] + J.n_starts;
   }
@@ -718,34 +781,58 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     }
     D.out = o_off[j] != ~0ull ? wout_.as<int32_t>() + o_off[j] : J.out;
   }
+  if (mode == BINGO_WALK_BATCHED && prefix[n_jobs] >= (1ull << 32))
+    throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one batched call");
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const uint64_t per = jobs[j].app == BINGO_SAMPLING ? 1 : jobs[j].length;
+    if (jobs[j].n_starts * per >= (32ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "job output exceeds 2^35 entries");
+    if (o_off[j] == ~0ull && jobs[j].app != BINGO_SAMPLING && (reinterpret_cast<uintptr_t>(jobs[j].out) & 31))
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "device output must be 32-byte aligned");
+  }
   const WalkView W = wview();
+  queue_.ensure(4 * std::max<uint32_t>(n_jobs, 1), "walk queue");
+  uint32_t* q = queue_.as<uint32_t>();
   if (mode == BINGO_WALK_PLAIN) {
+    // One launch per job, each with its own work counter.
+    cuda_check(cudaMemsetAsync(q, 0, 4 * n_jobs, stream_), "queue reset");
     for (uint32_t j = 0; j < n_jobs; ++j) {
       if (!dj[j].n) continue;
-      const unsigned g = grid_for(dj[j].n, kBlock, 8);
+      const unsigned long long nw = dj[j].n;
       switch (dj[j].app) {
-        case APP_DEEPWALK: k_walk_plain<APP_DEEPWALK><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
-        case APP_NODE2VEC: k_walk_plain<APP_NODE2VEC><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
-        case APP_PPR: k_walk_plain<APP_PPR><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
-        default: k_walk_plain<APP_SAMPLING><<<g, kBlock, 0, stream_>>>(W, dj[j]); break;
+        case APP_DEEPWALK:
+          k_walk<APP_DEEPWALK><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK>()), kBlock, 0, stream_>>>(
+              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          break;
+        case APP_NODE2VEC:
+          k_walk<APP_NODE2VEC><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC>()), kBlock, 0, stream_>>>(
+              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          break;
+        case APP_PPR:
+          k_walk<APP_PPR><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR>()), kBlock, 0, stream_>>>(
+              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          break;
+        default:
+          k_walk<APP_SAMPLING><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING>()), kBlock, 0, stream_>>>(
+              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          break;
       }
       cuda_check(cudaGetLastError(), "walk launch");
-  ++launches_;
+      ++launches_;
     }
   } else if (prefix[n_jobs]) {
     jobs_.ensure(n_jobs * sizeof(WalkJobDev), "walk jobs");
-    prefix_.ensure((n_jobs + 1) * 8, "walk jobs");
-    queue_.ensure(8, "walk queue");
+    prefix_.ensure((n_jobs + 1) * 4, "walk jobs");
+    std::vector<uint32_t> p32(prefix.begin(), prefix.end());
     cuda_check(cudaMemcpyAsync(jobs_.p, dj.data(), n_jobs * sizeof(WalkJobDev), cudaMemcpyHostToDevice, stream_),
                "jobs H2D");
-    cuda_check(cudaMemcpyAsync(prefix_.p, prefix.data(), (n_jobs + 1) * 8, cudaMemcpyHostToDevice, stream_),
+    cuda_check(cudaMemcpyAsync(prefix_.p, p32.data(), (n_jobs + 1) * 4, cudaMemcpyHostToDevice, stream_),
                "prefix H2D");
-    cuda_check(cudaMemsetAsync(queue_.p, 0, 8, stream_), "queue reset");
-    const unsigned g = grid_for(prefix[n_jobs], kBlock, 8);
-    k_walk_batched<<<g, kBlock, 0, stream_>>>(W, jobs_.as<WalkJobDev>(), prefix_.as<unsigned long long>(), n_jobs,
-                                               prefix[n_jobs], queue_.as<unsigned long long>());
+    cuda_check(cudaMemsetAsync(q, 0, 4, stream_), "queue reset");
+    const unsigned g = grid_for(prefix[n_jobs], kBlock, walk_blocks_per_sm<-1>());
+    k_walk<-1><<<g, kBlock, 0, stream_>>>(W, dj[0], jobs_.as<WalkJobDev>(), prefix_.as<uint32_t>(), n_jobs,
+                                          (uint32_t)prefix[n_jobs], q);
     cuda_check(cudaGetLastError(), "walk launch");
-  ++launches_;
+    ++launches_;
   }
   for (uint32_t j = 0; j < n_jobs; ++j)
     if (o_off[j] != ~0ull) {

@@ -299,41 +299,64 @@ __device__ __forceinline__ void plan_append(const StoreView& S, uint32_t u, cons
 }
 
 // ---------------------------------------------------------------------------
-// Delete a run of slots of one vertex in order: swap-remove the slot from
-// each of its groups (lane k = group k), tombstone it, then rebuild the alias
-// table. Replaces NodeData::deleteE (include/Bingo.cuh:199-218) and the
-// tombstone loop of deleteKernel (include/operation.cuh:209-210).
-static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32_t* seg_slot, uint32_t len) {
+// Delete a run of slots of one vertex in batch order. Each delete swap-removes
+// the slot from every group its weight has a bit in (lane k = group k) and
+// then tombstones the slot. Groups are independent, so each lane walks its
+// own sequence of removals with no warp synchronisation per delete; the
+// slot records of 32 deletes are fetched at once and the tombstones of a
+// chunk are written after its removals (the reference also tombstones after
+// its removal loop, include/operation.cuh:206-210). A delete is skipped and
+// counted when its slot is out of range, already a tombstone, or repeats an
+// earlier delete of the batch. Replaces NodeData::deleteE
+// (include/Bingo.cuh:199-218) and deleteKernel (include/operation.cuh:198-214).
+// stage: 64 words of shared memory owned by this warp.
+static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32_t* seg_slot, uint32_t len,
+                                    uint32_t* stage) {
   const int lane = threadIdx.x & 31;
+  const uint32_t below = lanemask_lt();
   VertexMeta M = S.meta[u];
   GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
   VertexRec R = S.vrec[u];
+  const size_t gb = (size_t)G.base * 4;
   uint32_t rejected = 0;
-  for (uint32_t d = 0; d < len; ++d) {
-    const uint32_t slot = seg_slot[d];
+  for (uint32_t c = 0; c < len; c += 32) {
+    const uint32_t i = c + lane;
+    const uint32_t slot = i < len ? seg_slot[i] : 0xffffffffu;
     EdgeRec e{0, 0, 0, 0};
-    if (slot < M.ecnt) e = S.edges[M.eoff + slot];
-    if (e.w == 0) {
-      ++rejected;
-      continue;
+    if (i < len && slot < M.ecnt) e = S.edges[M.eoff + slot];
+    const bool dup = (__match_any_sync(kFull, slot) & below) != 0;
+    const bool valid = i < len && e.w != 0 && !dup;
+    const uint32_t vmask = __ballot_sync(kFull, valid);
+    rejected += __popc(__ballot_sync(kFull, i < len && !valid));
+    stage[lane] = valid ? e.w : 0u;
+    stage[32 + lane] = e.ebp;
+    __syncwarp();
+    // This lane's removals, in batch order: the chunk's deletes with bit `lane`.
+    uint32_t mine = 0;
+    for (uint32_t r = vmask; r; r &= r - 1) {
+      const int d = __ffs(r) - 1;
+      if ((stage[d] >> lane) & 1u) mine |= 1u << d;
     }
-    if ((e.w >> lane) & 1u) {
-      const size_t gb = (size_t)G.base * 4;
-      const uint32_t pos = S.bp[M.bpoff + e.ebp + __popc(e.w & lanemask_lt())];
+    while (mine) {
+      const int d = __ffs(mine) - 1;
+      mine &= mine - 1;
+      const uint32_t w = stage[d], ebp = stage[32 + d];
+      const uint32_t pos = S.bp[M.bpoff + ebp + __popc(w & below)];
       const uint32_t last = G.cnt - 1;
       const uint32_t ms = S.gs[gb + last];
-      S.gv[gb + pos] = S.gv[gb + last];
+      const uint32_t mv = S.gv[gb + last];
+      S.gv[gb + pos] = mv;
       S.gs[gb + pos] = ms;
       const EdgeRec em = S.edges[M.eoff + ms];
-      S.bp[M.bpoff + em.ebp + __popc(em.w & lanemask_lt())] = pos;
+      S.bp[M.bpoff + em.ebp + __popc(em.w & below)] = pos;
       G.cnt = last;
     }
     __syncwarp();
-    if (lane == 0) {
+    if (valid) {
       S.edges[M.eoff + slot].w = 0u;
       if (S.node2vec && R.hmask) hash_sub(S.hash + R.hoff, R.hmask, e.v);
     }
-    --M.live;
+    M.live -= __popc(vmask);
     __syncwarp();
   }
   if (rejected && lane == 0) {

@@ -134,6 +134,160 @@ __device__ __forceinline__ uint32_t run_walk_any(const WalkView& W, const WalkJo
   }
 }
 
+// ---------------------------------------------------------------------------
+// Step-at-a-time form for the persistent kernels: a lane advances its walk
+// one step per iteration and pulls a new walk as soon as its walk ends, so
+// dead-ended and early-stopped walks do not idle their warp. Same counters,
+// same outputs as run_walk.
+//
+// Row output goes through an 8-entry (one 32-byte sector) staging buffer per
+// lane in shared memory: a lane writes its row a whole sector at a time with
+// streaming (evict-first) stores, so the write-once walk output neither
+// lands in L2 as partial sectors nor evicts graph data.
+struct RowStage {
+  uint32_t sec;   // index of the buffered 32-byte sector within the job output; kNoSec: empty
+  uint32_t lohi;  // valid entries [lo, hi) of the sector: lo | hi << 8
+};
+constexpr uint32_t kNoSec = 0xffffffffu;
+
+// This lane's 8 staging entries (16-byte aligned, blockDim.x rows of 8).
+__device__ __forceinline__ int32_t* stage_buf(int32_t (*obuf)[8]) { return obuf[threadIdx.x]; }
+
+__device__ __forceinline__ void stage_flush(RowStage& o, int32_t* out, int32_t (*obuf)[8]) {
+  if (o.sec == kNoSec) return;
+  const int32_t* buf = stage_buf(obuf);
+  int32_t* sec = out + (size_t)o.sec * 8;
+  const uint32_t lo = o.lohi & 0xff, hi = o.lohi >> 8;
+  if (lo == 0 && hi == 8) {
+    const int4* b = reinterpret_cast<const int4*>(buf);
+    __stcs(reinterpret_cast<int4*>(sec), b[0]);
+    __stcs(reinterpret_cast<int4*>(sec) + 1, b[1]);
+  } else {
+    for (uint32_t t = lo; t < hi; ++t) __stcs(sec + t, buf[t]);
+  }
+  o.sec = kNoSec;
+}
+
+// Writes v to out[g] through the stage; a row's positions arrive in
+// non-decreasing order (PPR tail mode rewrites the last one). Job outputs are
+// 32-byte aligned, so sectors are counted from out.
+__device__ __forceinline__ void stage_put(RowStage& o, int32_t* out, int32_t (*obuf)[8], unsigned long long g,
+                                          int32_t v) {
+  const uint32_t sec = (uint32_t)(g >> 3), t = (uint32_t)(g & 7);
+  if (sec != o.sec) {
+    stage_flush(o, out, obuf);
+    o.sec = sec;
+    o.lohi = t | (t << 8);
+  }
+  stage_buf(obuf)[t] = v;
+  if (t + 1 > (o.lohi >> 8)) o.lohi = (o.lohi & 0xff) | ((t + 1) << 8);
+}
+
+// Pads out[g, g_end) with -1: the open sector through the stage, then whole
+// sectors with two 16-byte streaming stores each.
+__device__ __forceinline__ void stage_pad(RowStage& o, int32_t* out, int32_t (*obuf)[8], unsigned long long g,
+                                          unsigned long long g_end) {
+  for (; g < g_end && (g & 7); ++g) stage_put(o, out, obuf, g, -1);
+  stage_flush(o, out, obuf);
+  const int4 m1 = make_int4(-1, -1, -1, -1);
+  for (; g + 8 <= g_end; g += 8) {
+    __stcs(reinterpret_cast<int4*>(out + g), m1);
+    __stcs(reinterpret_cast<int4*>(out + g) + 1, m1);
+  }
+  for (; g < g_end; ++g) __stcs(out + g, -1);
+}
+
+struct LaneWalk {
+  uint32_t i;      // walk index within its job
+  uint32_t j;      // step being produced
+  uint32_t cur;    // current vertex
+  uint32_t pos;    // last row position written
+  int32_t prev;    // previous vertex (node2vec), -1 before the first move
+  uint32_t phoff;  // previous vertex's adjacency index (node2vec)
+  uint32_t phmask;
+};
+
+// Starts walk i; returns true if it still has steps to produce. Sampling jobs
+// complete here.
+template <int APP>
+__device__ __forceinline__ bool walk_begin(const WalkView& W, const WalkJobDev& J, uint32_t i, LaneWalk& s,
+                                           RowStage& o, int32_t (*obuf)[8], uint32_t& moves) {
+  const uint32_t start = J.starts ? J.starts[i] : J.first + i;
+  if (APP == APP_SAMPLING) {
+    int32_t x = -1;
+    if (start < W.n) {
+      const VertexRec R = load_vrec(W, start);
+      if (R.m) x = (int32_t)sample_at(W, R, philox(i, 1, 0, J.job, J.k0, J.k1));
+    } else {
+      set_err(W.err, E_RANGE);
+    }
+    J.out[i] = x;
+    moves += x >= 0;
+    return false;
+  }
+  const uint32_t L = J.L;
+  if (L == 0) return false;
+  const unsigned long long g0 = (unsigned long long)i * L;
+  if (start >= W.n) {
+    set_err(W.err, E_RANGE);
+    stage_pad(o, J.out, obuf, g0, g0 + L);
+    return false;
+  }
+  stage_put(o, J.out, obuf, g0, (int32_t)start);
+  s.i = i;
+  s.j = 1;
+  s.cur = start;
+  s.pos = 0;
+  s.prev = -1;
+  const bool tail = APP == APP_PPR && (J.flags & kWalkPprTail);
+  if (L > 1 || tail) return true;
+  stage_flush(o, J.out, obuf);
+  return false;
+}
+
+// Produces one step; returns false when the walk has ended (row padded and
+// flushed).
+template <int APP>
+__device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev& J, LaneWalk& s, RowStage& o,
+                                             int32_t (*obuf)[8], uint32_t& moves) {
+  const uint32_t L = J.L;
+  const bool tail = APP == APP_PPR && (J.flags & kWalkPprTail);
+  s.pos = s.j < L ? s.j : L - 1;
+  const unsigned long long g0 = (unsigned long long)s.i * L;
+  const VertexRec R = load_vrec(W, s.cur);
+  bool done = false;
+  if (!R.m) {
+    stage_put(o, J.out, obuf, g0 + s.pos, -1);
+    done = true;
+  } else {
+    uint32_t x;
+    if (APP == APP_NODE2VEC && s.prev >= 0) {
+      for (uint32_t t = 0;; ++t) {
+        x = sample_at(W, R, philox(s.i, s.j, 2 * t, J.job, J.k0, J.k1));
+        const unsigned long long thr =
+            (int32_t)x == s.prev ? J.thr_ret : (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
+        const uint32_t a = philox(s.i, s.j, 2 * t + 1, J.job, J.k0, J.k1).x;
+        if ((unsigned long long)a < thr || t + 1 == kMaxNode2vecTrials) break;
+      }
+    } else {
+      x = sample_at(W, R, philox(s.i, s.j, 0, J.job, J.k0, J.k1));
+    }
+    stage_put(o, J.out, obuf, g0 + s.pos, (int32_t)x);
+    ++moves;
+    if (APP == APP_NODE2VEC) {
+      s.prev = (int32_t)s.cur;
+      s.phoff = R.hoff;
+      s.phmask = R.hmask;
+    }
+    s.cur = x;
+    if (APP == APP_PPR && (unsigned long long)philox(s.i, s.j, 1, J.job, J.k0, J.k1).x < J.thr_stop) done = true;
+    ++s.j;
+    if ((s.j >= L && !tail) || (tail && s.j >= kMaxPprSteps)) done = true;
+  }
+  if (done) stage_pad(o, J.out, obuf, g0 + s.pos + 1, g0 + L);
+  return !done;
+}
+
 // One atomic per warp: adds the warp's produced steps to the running count.
 __device__ __forceinline__ void add_steps(const WalkView& W, unsigned long long mine) {
 #pragma unroll

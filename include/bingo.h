@@ -79,7 +79,8 @@ typedef struct bingo_walk_job {
   double p, q;            /* node2vec return / in-out parameters (reference P=0.5, Q=2) */
   double stop_prob;       /* PPR termination probability (reference TP=0.0125) */
   int32_t* out;           /* [n_starts][length] vertex ids, -1 after a dead end or stop;
-                             sampling: [n_starts] */
+                             sampling: [n_starts]. Device outputs of walk apps must be
+                             32-byte aligned (rows are written a sector at a time). */
 } bingo_walk_job;
 
 typedef struct bingo_stats {
