@@ -182,32 +182,6 @@ class CpuRun:
                     walk_steps_per_s=steps / t_walk, edge_updates_per_s=(len(ins[0]) + len(dels[0])) / t_upd)
 
 
-def gather_ceiling(dev, gib: float = 4.0, reps: int = 5):
-    """Random-sector read ceiling of this GPU: a torch gather of 4-byte words
-    at uniformly random indices over a table larger than L2. Each index costs
-    one random 32-byte DRAM sector (plus 12 sequential bytes of index and
-    output). Returns sector GB/s (32 B per random read) and reads/s."""
-    import torch
-    n = int(gib * (1 << 30)) // 4
-    table = torch.zeros(n, dtype=torch.int32, device=dev)
-    k = 1 << 27
-    idx = torch.randint(0, n, (k,), device=dev, dtype=torch.int64)
-    out = torch.empty(k, dtype=torch.int32, device=dev)
-    torch.index_select(table, 0, idx, out=out)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    best = 1e9
-    for _ in range(reps):
-        e0.record()
-        torch.index_select(table, 0, idx, out=out)
-        e1.record()
-        torch.cuda.synchronize(dev)
-        best = min(best, e0.elapsed_time(e1) / 1e3)
-    del table, idx, out
-    return {"random_sector_gbs": k * 32 / best / 1e9, "random_reads_per_s": k / best,
-            "total_gbs": k * (32 + 12) / best / 1e9, "table_gib": gib}
-
-
 def run_reference(args):
     """The reference arm: the reference has no CPU implementation of the path,
     so the CPU oracle port (OpenMP, all host threads) stands in for it, on the
@@ -380,7 +354,10 @@ def run_ours(args):
             "kernel": "k_walk_plain<DEEPWALK>", "bytes_per_step": BYTES_PER_STEP}
 
     if args.gather_ceiling:
-        roof["random_sector_ceiling"] = gather_ceiling(dev)
+        pr = g.probe_gather(4 << 30)
+        pr["independent_gbs"] = pr["independent_sectors_per_s"] * 32 / 1e9
+        pr["chain_gbs"] = pr["chain_sectors_per_s"] * 32 / 1e9
+        roof["random_sector_ceiling"] = pr
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r = CpuRun(n, src, dst, w).step(batches[0], args.cpu_walks, seed=7)

@@ -73,6 +73,7 @@ SIGNATURES = {
     "bingo_dump_sizes": (c_int, [c_void_p, POINTER(c_uint64)]),
     "bingo_dump_state": (c_int, [c_void_p] + [c_void_p] * 13),
     "bingo_philox": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
+    "bingo_probe_gather": (c_int, [c_void_p, c_uint64, c_void_p]),
     "bingo_gen_rmat": (c_uint64, [c_uint32, c_uint32, c_double, c_double, c_double, c_uint64, c_void_p, c_void_p]),
     "bingo_gen_weights": (None, [c_uint64, c_int, c_double, c_double, c_double, c_uint64, c_void_p]),
     "bingo_updgen_create": (c_void_p, [c_uint32, c_void_p, c_void_p, c_uint64, c_uint64]),

@@ -140,6 +140,11 @@ int bingo_dump_state(bingo_handle* h, uint32_t* ecnt, uint32_t* live, uint32_t* 
   });
 }
 
+int bingo_probe_gather(bingo_handle* h, uint64_t table_bytes, double out[3]) {
+  if (!out || table_bytes < (1u << 20)) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) { bingo::probe_gather(e.stream(), table_bytes, out); });
+}
+
 int bingo_philox(bingo_handle* h, const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4) {
   return guarded(h, [&](bingo::Engine& e) { e.philox_batch(ctr4, count, key, out4); });
 }

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.cuh"
@@ -786,10 +787,20 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const uint64_t per = jobs[j].app == BINGO_SAMPLING ? 1 : jobs[j].length;
     if (jobs[j].n_starts * per >= (32ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "job output exceeds 2^35 entries");
-    if (o_off[j] == ~0ull && jobs[j].app != BINGO_SAMPLING && (reinterpret_cast<uintptr_t>(jobs[j].out) & 31))
+    if (jobs[j].n_starts && o_off[j] == ~0ull && jobs[j].app != BINGO_SAMPLING &&
+        (reinterpret_cast<uintptr_t>(jobs[j].out) & 31))
       throw Error(BINGO_ERR_INVALID_ARGUMENT, "device output must be 32-byte aligned");
   }
   const WalkView W = wview();
+  auto launch = [&](auto kern, unsigned grid, const WalkJobDev& J0, const WalkJobDev* jb, const uint32_t* pf,
+                    uint32_t nj, uint32_t tot, uint32_t* qq) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(kBlock);
+    lc.stream = stream_;
+    cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq), "walk launch");
+    ++launches_;
+  };
   queue_.ensure(4 * std::max<uint32_t>(n_jobs, 1), "walk queue");
   uint32_t* q = queue_.as<uint32_t>();
   if (mode == BINGO_WALK_PLAIN) {
@@ -797,27 +808,25 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     cuda_check(cudaMemsetAsync(q, 0, 4 * n_jobs, stream_), "queue reset");
     for (uint32_t j = 0; j < n_jobs; ++j) {
       if (!dj[j].n) continue;
-      const unsigned long long nw = dj[j].n;
+      const uint32_t nw = (uint32_t)dj[j].n;
       switch (dj[j].app) {
         case APP_DEEPWALK:
-          k_walk<APP_DEEPWALK><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK>()), kBlock, 0, stream_>>>(
-              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          launch(k_walk<APP_DEEPWALK>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK>()), dj[j], nullptr,
+                 nullptr, 0, nw, q + j);
           break;
         case APP_NODE2VEC:
-          k_walk<APP_NODE2VEC><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC>()), kBlock, 0, stream_>>>(
-              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          launch(k_walk<APP_NODE2VEC>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC>()), dj[j], nullptr,
+                 nullptr, 0, nw, q + j);
           break;
         case APP_PPR:
-          k_walk<APP_PPR><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR>()), kBlock, 0, stream_>>>(
-              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          launch(k_walk<APP_PPR>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR>()), dj[j], nullptr, nullptr, 0,
+                 nw, q + j);
           break;
         default:
-          k_walk<APP_SAMPLING><<<grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING>()), kBlock, 0, stream_>>>(
-              W, dj[j], nullptr, nullptr, 0, (uint32_t)nw, q + j);
+          launch(k_walk<APP_SAMPLING>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING>()), dj[j], nullptr,
+                 nullptr, 0, nw, q + j);
           break;
       }
-      cuda_check(cudaGetLastError(), "walk launch");
-      ++launches_;
     }
   } else if (prefix[n_jobs]) {
     jobs_.ensure(n_jobs * sizeof(WalkJobDev), "walk jobs");
@@ -828,11 +837,8 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     cuda_check(cudaMemcpyAsync(prefix_.p, p32.data(), (n_jobs + 1) * 4, cudaMemcpyHostToDevice, stream_),
                "prefix H2D");
     cuda_check(cudaMemsetAsync(q, 0, 4, stream_), "queue reset");
-    const unsigned g = grid_for(prefix[n_jobs], kBlock, walk_blocks_per_sm<-1>());
-    k_walk<-1><<<g, kBlock, 0, stream_>>>(W, dj[0], jobs_.as<WalkJobDev>(), prefix_.as<uint32_t>(), n_jobs,
-                                          (uint32_t)prefix[n_jobs], q);
-    cuda_check(cudaGetLastError(), "walk launch");
-    ++launches_;
+    launch(k_walk<-1>, grid_for(prefix[n_jobs], kBlock, walk_blocks_per_sm<-1>()), dj[0],
+           jobs_.as<WalkJobDev>(), prefix_.as<uint32_t>(), n_jobs, (uint32_t)prefix[n_jobs], q);
   }
   for (uint32_t j = 0; j < n_jobs; ++j)
     if (o_off[j] != ~0ull) {

@@ -53,6 +53,7 @@ class Engine {
   void philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
 
   std::string last_error;
+  cudaStream_t stream() const { return stream_; }
 
  private:
   bingo_config cfg_;
@@ -93,5 +94,6 @@ class Engine {
 };
 
 bool is_device_ptr(const void* p);
+void probe_gather(cudaStream_t st, uint64_t table_bytes, double out[3]);
 
 }  // namespace bingo

@@ -210,6 +210,14 @@ class Graph:
                                          ctypes.c_void_p(out.ctypes.data)))
         return out
 
+    def probe_gather(self, table_bytes: int = 4 << 30) -> dict:
+        """Random 32-byte-sector read rates of this GPU (independent and
+        dependent-chain forms) and the dependent-read latency."""
+        out = np.zeros(3, np.float64)
+        self._check(self._L.bingo_probe_gather(self._h, table_bytes, ctypes.c_void_p(out.ctypes.data)))
+        return {"independent_sectors_per_s": float(out[0]), "chain_sectors_per_s": float(out[1]),
+                "chain_latency_ns": float(out[2]), "table_bytes": table_bytes}
+
     # ---------------------------------------------- reference-named aliases
     def build(self, src, dst, w, n: int):
         """Alias of load_edges under the reference's name (include/operation.cuh:33)."""

@@ -160,6 +160,13 @@ int bingo_dump_state(bingo_handle* h, uint32_t* ecnt, uint32_t* live, uint32_t* 
  * checking the walk random stream: out[4*i..4*i+3] = philox(ctr_i, key). */
 int bingo_philox(bingo_handle* h, const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
 
+/* Diagnostic with no counterpart in the reference: measures this GPU's
+ * random 32-byte-sector read rate from a table of table_bytes (allocated and
+ * freed by the call). out[0] = sectors/s with 8 independent reads in flight
+ * per thread, out[1] = sectors/s of dependent read chains (one per thread,
+ * the shape of a walk step), out[2] = mean dependent-read latency in ns. */
+int bingo_probe_gather(bingo_handle* h, uint64_t table_bytes, double out[3]);
+
 #ifdef __cplusplus
 }
 #endif
