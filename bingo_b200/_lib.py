@@ -67,6 +67,7 @@ SIGNATURES = {
     "bingo_insert_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
     "bingo_delete_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "bingo_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32, c_uint32]),
+    "bingo_walk_noalloc": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32]),
     "bingo_sync": (c_int, [c_void_p]),
     "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
     "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),

@@ -112,6 +112,10 @@ int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uin
   return guarded(h, [&](bingo::Engine& e) { e.walk(jobs, n_jobs, mode); });
 }
 
+int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs) {
+  return guarded(h, [&](bingo::Engine& e) { e.walk_noalloc(jobs, n_jobs); });
+}
+
 int bingo_sync(bingo_handle* h) {
   int st = BINGO_OK;
   const int g = guarded(h, [&](bingo::Engine& e) { st = e.sync(); });

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "engine.cuh"
 #include "store.cuh"
@@ -847,6 +848,106 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
                                  cudaMemcpyDeviceToHost, stream_),
                  "walk D2H");
     }
+  finish_call();
+}
+
+// ------------------------------------------------------------------ no-alloc walks
+// Scratch of bingo_walk_noalloc: job table, walk prefix and work counter in a
+// file-scope device array (every GPU that loads the library holds it until
+// exit). Host code reaches it only through the address cudaGetSymbolAddress
+// returns for the current device.
+constexpr uint32_t kNoAllocMaxJobs = 64;
+struct NoAllocScratch {
+  WalkJobDev jobs[kNoAllocMaxJobs];
+  uint32_t prefix[kNoAllocMaxJobs + 1];
+  uint32_t queue;
+};
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+namespace {
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_ptr[128] = {};
+
+// Device address of the scratch for `device` (must be current); looked up
+// once per device.
+NoAllocScratch* noalloc_scratch(int device) {
+  if (device < 0 || device >= 128) throw Error(BINGO_ERR_INVALID_ARGUMENT, "device ordinal above 127");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+    g_noalloc_ptr[device] = static_cast<NoAllocScratch*>(p);
+  }
+  return g_noalloc_ptr[device];
+}
+}  // namespace
+
+void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
+  require_loaded();
+  if (n_jobs == 0) return;
+  if (!jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
+  if (n_jobs > kNoAllocMaxJobs)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "bingo_walk_noalloc takes at most " + std::to_string(kNoAllocMaxJobs) +
+                                                " jobs per call (got " + std::to_string(n_jobs) + ")");
+  NoAllocScratch* scratch = noalloc_scratch(cfg_.device);
+  WalkJobDev dj[kNoAllocMaxJobs];
+  uint32_t prefix[kNoAllocMaxJobs + 1];
+  prefix[0] = 0;
+  uint64_t total = 0;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const bingo_walk_job& J = jobs[j];
+    if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
+    if (J.app == BINGO_NODE2VEC && !cfg_.node2vec)
+      throw Error(BINGO_ERR_UNSUPPORTED, "node2vec needs the adjacency index (config.node2vec)");
+    if (J.app == BINGO_NODE2VEC && !(J.p > 0 && J.q > 0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "p, q must be > 0");
+    if (J.app == BINGO_PPR && !(J.stop_prob >= 0 && J.stop_prob <= 1))
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "stop_prob must be in [0, 1]");
+    if (J.app != BINGO_SAMPLING && J.length == 0 && J.n_starts)
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "length must be >= 1");
+    if (J.n_starts) {
+      if (!J.out || !is_device_ptr(J.out))
+        throw Error(BINGO_ERR_INVALID_ARGUMENT, "bingo_walk_noalloc needs device output buffers");
+      if (J.starts && !is_device_ptr(J.starts))
+        throw Error(BINGO_ERR_INVALID_ARGUMENT, "bingo_walk_noalloc needs device start arrays (or NULL)");
+      if (J.app != BINGO_SAMPLING && (reinterpret_cast<uintptr_t>(J.out) & 31))
+        throw Error(BINGO_ERR_INVALID_ARGUMENT, "device output must be 32-byte aligned");
+      if (!J.starts && (uint64_t)J.first + J.n_starts > n_) throw Error(BINGO_ERR_OUT_OF_RANGE, "start range exceeds n");
+    }
+    total += J.n_starts;
+    if (total >= (1ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one call");
+    prefix[j + 1] = (uint32_t)total;
+    WalkJobDev& D = dj[j];
+    D.app = J.app;
+    D.L = J.length;
+    D.starts = J.starts;
+    D.n = J.n_starts;
+    D.first = J.first;
+    D.job = J.job_id;
+    D.k0 = (uint32_t)J.seed;
+    D.k1 = (uint32_t)(J.seed >> 32);
+    D.flags = J.flags;
+    D.pad = 0;
+    const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
+    const double wmax = std::max(wr, std::max(1.0, wo));
+    D.thr_ret = prob_threshold(wr / wmax);
+    D.thr_in = prob_threshold(1.0 / wmax);
+    D.thr_out = prob_threshold(wo / wmax);
+    D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+    D.out = J.out;
+  }
+  if (!total) return;
+  // The job table and prefix are copied from pageable host memory (the copy
+  // completes before the call returns); the work counter starts at zero.
+  cuda_check(cudaMemcpyAsync(scratch->jobs, dj, n_jobs * sizeof(WalkJobDev), cudaMemcpyHostToDevice, stream_),
+             "no-alloc jobs H2D");
+  cuda_check(cudaMemcpyAsync(scratch->prefix, prefix, (n_jobs + 1) * 4, cudaMemcpyHostToDevice, stream_),
+             "no-alloc prefix H2D");
+  cuda_check(cudaMemsetAsync(&scratch->queue, 0, 4, stream_), "no-alloc counter reset");
+  const WalkView W = wview();
+  k_walk<-1><<<grid_for(total, kBlock, walk_blocks_per_sm<-1>()), kBlock, 0, stream_>>>(
+      W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue);
+  cuda_check(cudaGetLastError(), "no-alloc walk launch");
+  ++launches_;
   finish_call();
 }
 

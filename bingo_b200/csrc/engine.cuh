@@ -43,6 +43,7 @@ class Engine {
   void insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
   void erase(const uint32_t* u, const uint32_t* slot, uint64_t k);
   void walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
+  void walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs);
   int sync();  // returns a bingo_status
   void set_stream(void* s);
   void stats(bingo_stats* out);

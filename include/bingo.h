@@ -134,6 +134,26 @@ int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot,
  * BINGO_WALK_BATCHED or BINGO_WALK_PLAIN; both give identical results. */
 int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
 
+/* Allocation-free walks. No counterpart in the reference: this entry point
+ * exists for callers that must not allocate GPU memory while they run - for
+ * example a serving loop whose HBM is already budgeted to the graph, a caller
+ * capturing work into a CUDA graph (allocation calls are not allowed inside a
+ * capture), or an application that owns the device memory pool. It runs the
+ * same walks as bingo_walk(jobs, n_jobs, BINGO_WALK_BATCHED), with identical
+ * results, but takes its scratch (job table, walk offsets and work counter)
+ * from a fixed array compiled into the library instead of allocating it, and
+ * never calls cudaMalloc or cudaFree.
+ *
+ * Limits: at most 64 jobs per call (more returns BINGO_ERR_INVALID_ARGUMENT);
+ * every start array must be device memory or NULL and every output device
+ * memory (32-byte aligned for walk apps), since host buffers would need
+ * staging memory. The scratch array is shared by every call on a device and
+ * keeps the last call's contents; calls whose work overlaps on the GPU (two
+ * streams, or two handles on one device, at once) race on it, so issue them
+ * in order on one stream. The first call on each device looks up the array's
+ * device address; make that first call before any stream capture. */
+int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs);
+
 /* Waits for all queued work; returns the first device-detected error since
  * the previous bingo_sync (or BINGO_OK). */
 int bingo_sync(bingo_handle* h);
