@@ -36,15 +36,15 @@ BYTES_PER_STEP = 32  # algorithmic bytes per produced walk step (vertex 8, alias
 WORKLOAD = "plain-deepwalk-rmat20"
 
 
-def make_workload(steps_total: int):
+def make_workload(steps_total: int, w_hi: int = W_HI):
     from bingo_b200 import gen
     n = 1 << SCALE
     src, dst = gen.rmat(SCALE, EDGE_FACTOR, seed=GRAPH_SEED)
-    w = gen.weights(len(src), gen.W_LOGUNIFORM, W_LO, W_HI, seed=GRAPH_SEED + 1)
+    w = gen.weights(len(src), gen.W_LOGUNIFORM, W_LO, w_hi, seed=GRAPH_SEED + 1)
     ug = gen.UpdateGen(n, src, dst, seed=GRAPH_SEED + 2)
     batches = []
     for _ in range(steps_total):
-        ins = ug.inserts(BATCH_INS, gen.W_LOGUNIFORM, W_LO, W_HI)
+        ins = ug.inserts(BATCH_INS, gen.W_LOGUNIFORM, W_LO, w_hi)
         dels = ug.deletes(BATCH_DEL)
         batches.append((ins, dels))
     return n, src, dst, w, batches
@@ -214,6 +214,113 @@ def run_reference(args):
         "walk_steps_per_s": last["walk_steps_per_s"], "edge_updates_per_s": last["edge_updates_per_s"],
     }
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- reference CUDA build
+REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+
+def run_reference_cuda(args):
+    """The reference's own CUDA build (oracle/_ref/ref_harness, compiled from
+    the reference sources) on the same GPU, on this workload with weights
+    capped below 2^16 (its MAXLOG = 16 bit groups), next to this engine on
+    the identical input. The reference walks every vertex once per step with
+    its deepwalkKernel<<<512,128>>> (timed with CUDA events) and applies each
+    batch with its host insert()/deleteE() wrappers (timed on the host: they
+    sort, grow vertices and synchronise on the host by design)."""
+    import struct
+    import tempfile
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    if not os.path.exists(REF_HARNESS):
+        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/ref_harness not built "
+                          "(make -C oracle ref needs the reference sources)"}))
+        return
+    total = args.warmup + args.steps
+    w_hi = 1 << 16
+    n, src, dst, w, batches = make_workload(total, w_hi=w_hi)
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.bin")
+        with open(inp, "wb") as f:
+            f.write(b"BREF")
+            f.write(struct.pack("<IIQfI", 1, n, len(src), 0.4, 0))
+            f.write(np.stack([src, dst, w], 1).astype("<u4").tobytes())
+            for i, (ins, dels) in enumerate(batches):
+                f.write(struct.pack("<IQ", 1, len(ins[0])))
+                f.write(np.stack(ins, 1).astype("<u4").tobytes())
+                f.write(struct.pack("<IQ", 2, len(dels[0])))
+                f.write(np.stack(dels, 1).astype("<u4").tobytes())
+                f.write(struct.pack("<IIIQ", 4, 0, 1, 1000 + i))
+            f.write(struct.pack("<I", 0))
+        r = subprocess.run([REF_HARNESS, inp, "-"], capture_output=True, text=True, timeout=1800)
+    if r.returncode:
+        print(json.dumps({"impl": "reference-cuda", "unavailable": f"ref_harness exited {r.returncode}: "
+                          + r.stderr.strip().splitlines()[-1][:200] if r.stderr.strip() else "no message"}))
+        return
+    ops = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    ins_s = [o["wall_s"] for o in ops if o["op"] == "insert"][args.warmup:]
+    del_s = [o["wall_s"] for o in ops if o["op"] == "delete"][args.warmup:]
+    walks = [o for o in ops if o["op"] == "walk"][args.warmup:]
+    walk_s = sum(o["kernel_ms"] for o in walks) / 1e3
+    steps = sum(o["steps"] for o in walks)
+    ref = {"value": steps / (walk_s + sum(ins_s) + sum(del_s)), "walk_steps_per_s": steps / walk_s,
+           "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * len(walks) / (sum(ins_s) + sum(del_s)),
+           "walk_kernel_ms_per_step": walk_s * 1e3 / len(walks),
+           "update_wall_ms_per_step": (sum(ins_s) + sum(del_s)) * 1e3 / len(walks),
+           "steps_per_walk_phase": steps / len(walks)}
+    ours = measure_engine(args, n, src, dst, w, batches, local)
+    line = {"impl": "reference-cuda", "metric": "walk_steps_per_s", "value": ref["value"], "unit": "steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "config": {"workload": WORKLOAD + "-w16", "scale": SCALE, "edge_factor": EDGE_FACTOR,
+                       "weights": "loguniform[1,2^16)", "walks": n, "walk_len": WALK_LEN,
+                       "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}},
+            "reference": ref, "ours_same_input": ours}
+    print(json.dumps(line), flush=True)
+
+
+def measure_engine(args, n, src, dst, w, batches, local):
+    """This engine on the given workload: device-timed steps (inputs in HBM)."""
+    import torch
+    from bingo_b200 import DEEPWALK, PLAIN, Graph, WalkJob
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    g = Graph(device=local, synchronous=False)
+    g.set_stream(stream.cuda_stream)
+    g.load_edges(src, dst, w, n)
+
+    def dev_i32(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)
+
+    db = [((dev_i32(i[0]), dev_i32(i[1]), dev_i32(i[2])), (dev_i32(d[0]), dev_i32(d[1]))) for i, d in batches]
+    out = torch.empty((n, WALK_LEN), dtype=torch.int32, device=dev)
+    slots = torch.empty(BATCH_INS, dtype=torch.int32, device=dev)
+    total = args.warmup + args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(total)]
+    for i in range(total):
+        if i == args.warmup:
+            g.sync()
+            s0 = g.stats()["walk_steps"]
+        (a, b, c), (du, ds) = db[i]
+        ev[i][0].record(stream)
+        g.insert_batch(a, b, c, out_slots=slots)
+        g.delete_batch(du, ds)
+        ev[i][1].record(stream)
+        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, n_starts=n, first=0, job_id=i, seed=1, out=out)],
+                    mode=PLAIN)
+        ev[i][2].record(stream)
+    g.sync()
+    torch.cuda.synchronize(dev)
+    steps = g.stats()["walk_steps"] - s0
+    upd = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(args.warmup, total)) / 1e3
+    wlk = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
+    whole = sum(ev[i][0].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
+    g.close()
+    return {"value": steps / whole, "walk_steps_per_s": steps / wlk,
+            "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * args.steps / upd,
+            "walk_kernel_ms_per_step": wlk * 1e3 / args.steps, "update_ms_per_step": upd * 1e3 / args.steps,
+            "steps_per_walk_phase": steps / args.steps}
 
 
 # --------------------------------------------------------------------------- GPU arm
@@ -398,7 +505,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--cpu-walks", type=int, default=131072)
     ap.add_argument("--ref-walks", type=int, default=131072)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
@@ -410,6 +517,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference-cuda":
+        run_reference_cuda(args)
     else:
         run_ours(args)
 
