@@ -7,6 +7,6 @@ include/bingo.h. This package is the host-side mirror of the reference's
 operator interface (`Graph.build / insert / deleteE / walk`).
 """
 from ._lib import BingoError, LIB_PATH, lib  # noqa: F401
-from .engine import (APPS, BATCHED, DEEPWALK, NODE2VEC, PLAIN, PPR, SAMPLING, WALK_PPR_TAIL,  # noqa: F401
-                     Graph, WalkJob)
+from .engine import (APPS, BATCHED, DEEPWALK, NODE2VEC, PLAIN, PPR, RUN_GRAPH, SAMPLING,  # noqa: F401
+                     WALK_PPR_TAIL, Graph, WalkJob)
 from . import gen  # noqa: F401

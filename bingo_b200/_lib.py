@@ -42,6 +42,19 @@ class BingoWalkJob(ctypes.Structure):
     ]
 
 
+class BingoOp(ctypes.Structure):
+    _fields_ = [
+        ("kind", c_int32),
+        ("n_jobs", c_uint32),
+        ("jobs", POINTER(BingoWalkJob)),
+        ("a", c_void_p),
+        ("b", c_void_p),
+        ("c", c_void_p),
+        ("k", c_uint64),
+        ("out_slots", c_void_p),
+    ]
+
+
 class BingoStats(ctypes.Structure):
     _fields_ = [
         ("n", c_uint32),
@@ -68,6 +81,7 @@ SIGNATURES = {
     "bingo_delete_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "bingo_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32, c_uint32]),
     "bingo_walk_noalloc": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32]),
+    "bingo_run": (c_int, [c_void_p, POINTER(BingoOp), c_uint32, c_uint32]),
     "bingo_sync": (c_int, [c_void_p]),
     "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
     "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),

@@ -116,6 +116,10 @@ int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_j
   return guarded(h, [&](bingo::Engine& e) { e.walk_noalloc(jobs, n_jobs); });
 }
 
+int bingo_run(bingo_handle* h, const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
+  return guarded(h, [&](bingo::Engine& e) { e.run(ops, n_ops, flags); });
+}
+
 int bingo_sync(bingo_handle* h) {
   int st = BINGO_OK;
   const int g = guarded(h, [&](bingo::Engine& e) { st = e.sync(); });

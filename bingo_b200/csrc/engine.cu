@@ -360,6 +360,8 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
 Engine::~Engine() {
   cudaSetDevice(cfg_.device);
   if (stream_) cudaStreamSynchronize(stream_);
+  drop_graph();
+  prog_jobs_.release(), prog_prefix_.release(), prog_queue_.release();
   DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
                     &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
                     &prefix_, &queue_, &wstart_, &wout_};
@@ -524,6 +526,7 @@ void Engine::grow_arena(int a, unsigned long long min_cap) {
   arena_[a] = fresh;
   fresh.p = nullptr;
   cap_[a] = nc;
+  ++arena_gen_;
 }
 
 void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
@@ -557,6 +560,7 @@ void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
   }
   cuda_check(cudaMemsetAsync(d_top_, 0, kArenas * sizeof(unsigned long long), stream_), "reset tops");
   std::memset(h_top_, 0, kArenas * sizeof(unsigned long long));
+  ++arena_gen_;
 }
 
 // Plan, size, reserve and apply an append batch whose grouped columns are in
@@ -583,6 +587,9 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   uint32_t ctl = 0;
   cuda_check(cudaMemcpyAsync(tot, d_tot, sizeof tot, cudaMemcpyDeviceToHost, stream_), "read totals");
   cuda_check(cudaMemcpyAsync(&ctl, ctl_.p, 4, cudaMemcpyDeviceToHost, stream_), "read ctl");
+  if (!load_mode)
+    cuda_check(cudaMemcpyAsync(h_top_, d_top_, kArenas * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+               "read tops");
   cuda_check(cudaStreamSynchronize(stream_), "plan sync");
   if (ctl) {
     cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
@@ -630,6 +637,7 @@ void Engine::load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, u
   cuda_check(cudaStreamSynchronize(stream_), "load");
   loaded_ = false;
   n_ = n;
+  ++arena_gen_;
   vrec_.release(), meta_.release(), gdesc_.release();
   vrec_.ensure((size_t)n * sizeof(VertexRec), "vertex records");
   meta_.ensure((size_t)n * sizeof(VertexMeta), "vertex metadata");
@@ -849,6 +857,240 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
                  "walk D2H");
     }
   finish_call();
+}
+
+// ------------------------------------------------------------------ programs
+void Engine::drop_graph() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+  graph_sig_ = 0;
+}
+
+// Insert without host synchronisation: the batch's arena needs are reserved
+// on the device (all or nothing); a batch that does not fit is not applied
+// and raises E_CAPACITY. Inputs are device arrays.
+void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k,
+                            uint32_t* out_slots) {
+  const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(a, b, c, k, n_, ctl_.as<uint32_t>(), d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  group_by_vertex(a, b, c, k);
+  const StoreView S = view();
+  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
+      S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
+      ctl_.as<uint32_t>(), need_.as<unsigned long long>());
+  cuda_check(cudaGetLastError(), "plan");
+  ++launches_;
+  for (int ar = 0; ar < kArenas; ++ar) {
+    size_t tb = cub_tmp_.bytes;
+    cuda_check(cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tb, need_.as<unsigned long long>() + (size_t)ar * ks,
+                                             scan_.as<unsigned long long>() + (size_t)ar * ks, (int)ks, stream_),
+               "scan");
+  }
+  unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
+  k_totals<<<1, 32, 0, stream_>>>(need_.as<unsigned long long>(), scan_.as<unsigned long long>(), ks, d_tot);
+  cuda_check(cudaGetLastError(), "totals");
+  ++launches_;
+  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
+  cuda_check(cudaGetLastError(), "reserve");
+  ++launches_;
+  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+      S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
+      base_.as<unsigned long long>(), out_slots);
+  cuda_check(cudaGetLastError(), "apply insert");
+  ++launches_;
+}
+
+void Engine::enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k) {
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(u, nullptr, nullptr, k, n_, ctl_.as<uint32_t>(),
+                                                              d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  group_by_vertex(u, slot, nullptr, k);
+  const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
+  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+      view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
+      ctl_.as<uint32_t>());
+  cuda_check(cudaGetLastError(), "apply delete");
+  ++launches_;
+}
+
+// Grows arenas so that a program inserting k edges in total is unlikely to
+// run out on the device: free space >= a quarter of the used space plus a
+// per-edge allowance (every set bit may double its group, every slot its
+// vertex arrays).
+void Engine::ensure_headroom(uint64_t k_ins) {
+  static const unsigned long long per_edge[kArenas] = {64, 2, 64, 2, 4};
+  read_tops();
+  for (int a = 0; a < kArenas; ++a) {
+    if (a == A_HASH && !cfg_.node2vec) continue;
+    const unsigned long long want = h_top_[a] / 4 + per_edge[a] * k_ins + kArenaFloor[a];
+    if (cap_[a] - h_top_[a] < want) grow_arena(a, h_top_[a] + 2 * want);
+  }
+}
+
+void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
+  require_loaded();
+  if (n_ops == 0) return;
+  if (!ops) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null op array");
+  const bool use_graph = flags & BINGO_RUN_GRAPH;
+  // ---- validate, size scratch, lay out the job tables
+  uint64_t kmax = 0, k_ins = 0, n_jobs_total = 0, n_walk_ops = 0;
+  uint64_t sig = 1469598103934665603ull;
+  auto mix = [&](uint64_t x) { sig = (sig ^ x) * 1099511628211ull; };
+  for (uint32_t i = 0; i < n_ops; ++i) {
+    const bingo_op& o = ops[i];
+    mix((uint64_t)o.kind);
+    if (o.kind == BINGO_OP_INSERT || o.kind == BINGO_OP_DELETE) {
+      const bool ins = o.kind == BINGO_OP_INSERT;
+      if (!o.k) continue;
+      if (o.k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "batch larger than 2^31");
+      if (!o.a || !o.b || (ins && !o.c)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null batch array");
+      if (!is_device_ptr(o.a) || !is_device_ptr(o.b) || (ins && !is_device_ptr(o.c)) ||
+          (o.out_slots && !is_device_ptr(o.out_slots)))
+        throw Error(BINGO_ERR_INVALID_ARGUMENT, "program batches must be device arrays");
+      kmax = std::max<uint64_t>(kmax, o.k);
+      if (ins) k_ins += o.k;
+      mix(o.k), mix((uint64_t)(uintptr_t)o.a), mix((uint64_t)(uintptr_t)o.b), mix((uint64_t)(uintptr_t)o.c);
+      mix((uint64_t)(uintptr_t)o.out_slots);
+    } else if (o.kind == BINGO_OP_WALK) {
+      if (o.n_jobs && !o.jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
+      n_jobs_total += o.n_jobs;
+      ++n_walk_ops;
+      mix(o.n_jobs);
+      for (uint32_t j = 0; j < o.n_jobs; ++j) mix(o.jobs[j].n_starts);
+    } else {
+      throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown op kind");
+    }
+  }
+  if (kmax) ensure_batch_scratch(kmax);
+  ensure_headroom(k_ins);
+  mix(arena_gen_), mix(n_);
+  std::vector<WalkJobDev> dj;
+  std::vector<uint32_t> pf;
+  std::vector<uint64_t> job_off(n_ops, 0), pf_off(n_ops, 0), totals(n_ops, 0);
+  dj.reserve(n_jobs_total);
+  for (uint32_t i = 0; i < n_ops; ++i) {
+    const bingo_op& o = ops[i];
+    if (o.kind != BINGO_OP_WALK) continue;
+    job_off[i] = dj.size();
+    pf_off[i] = pf.size();
+    uint64_t t = 0;
+    pf.push_back(0);
+    for (uint32_t j = 0; j < o.n_jobs; ++j) {
+      const bingo_walk_job& J = o.jobs[j];
+      if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
+      if (J.app == BINGO_NODE2VEC && !cfg_.node2vec)
+        throw Error(BINGO_ERR_UNSUPPORTED, "node2vec needs the adjacency index (config.node2vec)");
+      if (J.app == BINGO_NODE2VEC && !(J.p > 0 && J.q > 0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "p, q must be > 0");
+      if (J.app == BINGO_PPR && !(J.stop_prob >= 0 && J.stop_prob <= 1))
+        throw Error(BINGO_ERR_INVALID_ARGUMENT, "stop_prob must be in [0, 1]");
+      if (J.n_starts) {
+        if (J.app != BINGO_SAMPLING && J.length == 0) throw Error(BINGO_ERR_INVALID_ARGUMENT, "length must be >= 1");
+        if (!J.out || !is_device_ptr(J.out)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "program outputs must be device arrays");
+        if (J.starts && !is_device_ptr(J.starts))
+          throw Error(BINGO_ERR_INVALID_ARGUMENT, "program start arrays must be device arrays");
+        if (J.app != BINGO_SAMPLING && (reinterpret_cast<uintptr_t>(J.out) & 31))
+          throw Error(BINGO_ERR_INVALID_ARGUMENT, "device output must be 32-byte aligned");
+        if (!J.starts && (uint64_t)J.first + J.n_starts > n_) throw Error(BINGO_ERR_OUT_OF_RANGE, "start range exceeds n");
+      }
+      t += J.n_starts;
+      if (t >= (1ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one op");
+      pf.push_back((uint32_t)t);
+      WalkJobDev D;
+      D.app = J.app;
+      D.L = J.length;
+      D.starts = J.starts;
+      D.n = J.n_starts;
+      D.first = J.first;
+      D.job = J.job_id;
+      D.k0 = (uint32_t)J.seed;
+      D.k1 = (uint32_t)(J.seed >> 32);
+      D.flags = J.flags;
+      D.pad = 0;
+      const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
+      const double wmax = std::max(wr, std::max(1.0, wo));
+      D.thr_ret = prob_threshold(wr / wmax);
+      D.thr_in = prob_threshold(1.0 / wmax);
+      D.thr_out = prob_threshold(wo / wmax);
+      D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+      D.out = J.out;
+      dj.push_back(D);
+    }
+    totals[i] = t;
+  }
+  // Job tables are read by the walk kernels from device memory, so their
+  // contents may change between replays of a captured program.
+  if (!dj.empty()) {
+    const size_t jb = dj.size() * sizeof(WalkJobDev), pb = pf.size() * 4;
+    if (jb > prog_jobs_.bytes || pb > prog_prefix_.bytes || n_walk_ops * 4 > prog_queue_.bytes) drop_graph();
+    prog_jobs_.ensure(jb, "program jobs");
+    prog_prefix_.ensure(pb, "program jobs");
+    prog_queue_.ensure(std::max<uint64_t>(n_walk_ops, 1) * 4, "program queue");
+    cuda_check(cudaMemcpyAsync(prog_jobs_.p, dj.data(), jb, cudaMemcpyHostToDevice, stream_), "program jobs H2D");
+    cuda_check(cudaMemcpyAsync(prog_prefix_.p, pf.data(), pb, cudaMemcpyHostToDevice, stream_), "program jobs H2D");
+  }
+  mix((uint64_t)(uintptr_t)prog_jobs_.p), mix((uint64_t)(uintptr_t)ctl_.p), mix((uint64_t)(uintptr_t)cub_tmp_.p);
+  mix(cub_tmp_.bytes);
+
+  const uint64_t launches0 = launches_;
+  auto enqueue_all = [&]() {
+    if (n_walk_ops) cuda_check(cudaMemsetAsync(prog_queue_.p, 0, n_walk_ops * 4, stream_), "program queue reset");
+    uint32_t wi = 0;
+    const WalkView W = wview();
+    for (uint32_t i = 0; i < n_ops; ++i) {
+      const bingo_op& o = ops[i];
+      if (o.kind == BINGO_OP_INSERT && o.k) {
+        enqueue_insert(o.a, o.b, o.c, o.k, o.out_slots);
+      } else if (o.kind == BINGO_OP_DELETE && o.k) {
+        enqueue_delete(o.a, o.b, o.k);
+      } else if (o.kind == BINGO_OP_WALK) {
+        uint32_t* q = prog_queue_.as<uint32_t>() + wi++;
+        if (!totals[i]) continue;
+        WalkJobDev* jt = prog_jobs_.as<WalkJobDev>() + job_off[i];
+        const uint32_t* pp = prog_prefix_.as<uint32_t>() + pf_off[i];
+        k_walk<-1><<<grid_for(totals[i], kBlock, walk_blocks_per_sm<-1>()), kBlock, 0, stream_>>>(
+            W, dj[job_off[i]], jt, pp, o.n_jobs, (uint32_t)totals[i], q);
+        cuda_check(cudaGetLastError(), "program walk launch");
+        ++launches_;
+      }
+    }
+  };
+  if (use_graph) {
+    if (!graph_exec_ || graph_sig_ != sig) {
+      drop_graph();
+      cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+      try {
+        enqueue_all();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+      }
+      cuda_check(cudaStreamEndCapture(stream_, &graph_), "end capture");
+      cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "instantiate graph");
+      graph_sig_ = sig;
+      graph_launches_ = launches_ - launches0;
+      launches_ = launches0;
+    }
+    cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+    launches_ += graph_launches_;
+  } else {
+    enqueue_all();
+  }
+  if (cfg_.synchronous) {
+    const int st = sync();
+    read_tops();
+    if (st) throw Error(st, last_error);
+  }
 }
 
 // ------------------------------------------------------------------ no-alloc walks

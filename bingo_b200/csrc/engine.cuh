@@ -44,6 +44,7 @@ class Engine {
   void erase(const uint32_t* u, const uint32_t* slot, uint64_t k);
   void walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
   void walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs);
+  void run(const bingo_op* ops, uint32_t n_ops, uint32_t flags);
   int sync();  // returns a bingo_status
   void set_stream(void* s);
   void stats(bingo_stats* out);
@@ -80,6 +81,12 @@ class Engine {
   uint64_t iota_n_ = 0;
   // walk scratch
   DevBuf jobs_, prefix_, queue_, wstart_, wout_;
+  // programs
+  DevBuf prog_jobs_, prog_prefix_, prog_queue_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  uint64_t graph_sig_ = 0, graph_launches_ = 0;
+  uint64_t arena_gen_ = 0;  // bumped whenever an arena or the vertex arrays are reallocated
 
   StoreView view() const;
   WalkView wview() const;
@@ -87,6 +94,10 @@ class Engine {
   const uint32_t* stage(const uint32_t* p, uint64_t k, DevBuf& buf, const char* what);
   void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k);
   void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
+  void enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k, uint32_t* out_slots);
+  void enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k);
+  void ensure_headroom(uint64_t k_insert_total);
+  void drop_graph();
   void alloc_arenas(const unsigned long long need[kArenas]);
   void grow_arena(int a, unsigned long long min_cap);
   void read_tops();

@@ -14,12 +14,14 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import BingoConfig, BingoError, BingoStats, BingoWalkJob, lib
+from ._lib import BingoConfig, BingoError, BingoOp, BingoStats, BingoWalkJob, lib
 
 DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
 WALK_PPR_TAIL = 1
 BATCHED, PLAIN = 0, 1
+OP_WALK, OP_INSERT, OP_DELETE = 0, 1, 2
+RUN_GRAPH = 1
 
 
 def _u32(a):
@@ -138,10 +140,9 @@ class Graph:
         psl, ksl = _u32(slot)
         self._check(self._L.bingo_delete_batch(self._h, pu, psl, k))
 
-    def walk_jobs(self, jobs: Sequence[WalkJob], mode: int = BATCHED):
-        """Run a list of walk jobs; each job's out must be preallocated."""
+    @staticmethod
+    def _job_array(jobs: Sequence[WalkJob], keep: list):
         arr = (BingoWalkJob * len(jobs))()
-        keep = []
         for i, j in enumerate(jobs):
             ps, ks = _u32(j.starts) if j.starts is not None else (None, None)
             po, ko = _out(j.out, np.int32)
@@ -158,7 +159,43 @@ class Graph:
             arr[i].q = j.q
             arr[i].stop_prob = j.stop_prob
             arr[i].out = po
+        return arr
+
+    def walk_jobs(self, jobs: Sequence[WalkJob], mode: int = BATCHED):
+        """Run a list of walk jobs; each job's out must be preallocated."""
+        keep = []
+        arr = self._job_array(jobs, keep)
         self._check(self._L.bingo_walk(self._h, arr, len(jobs), mode))
+
+    def run(self, ops: Sequence[tuple], graph: bool = True):
+        """Run a program: a list of ("walk", [WalkJob...]), ("insert", src, dst,
+        w[, out_slots]) and ("delete", u, slot) with device tensors, in order
+        and without host synchronisation (bingo_run). graph=True captures it
+        into a CUDA graph replayed while its shape is unchanged."""
+        arr = (BingoOp * len(ops))()
+        keep = []
+        for i, op in enumerate(ops):
+            kind = op[0]
+            if kind == "walk":
+                jobs = self._job_array(op[1], keep)
+                keep.append(jobs)
+                arr[i].kind, arr[i].n_jobs = OP_WALK, len(op[1])
+                arr[i].jobs = ctypes.cast(jobs, ctypes.POINTER(BingoWalkJob))
+            elif kind in ("insert", "delete"):
+                cols = [_u32(x) for x in op[1:4 if kind == "insert" else 3]]
+                keep += [c[1] for c in cols]
+                arr[i].kind = OP_INSERT if kind == "insert" else OP_DELETE
+                arr[i].a, arr[i].b = cols[0][0], cols[1][0]
+                if kind == "insert":
+                    arr[i].c = cols[2][0]
+                    if len(op) > 4 and op[4] is not None:
+                        po, ko = _out(op[4], np.uint32)
+                        keep.append(ko)
+                        arr[i].out_slots = po
+                arr[i].k = op[1].numel() if hasattr(op[1], "numel") else len(op[1])
+            else:
+                raise ValueError(f"unknown op {kind!r}")
+        self._check(self._L.bingo_run(self._h, arr, len(ops), RUN_GRAPH if graph else 0))
 
     def walk(self, app: int = DEEPWALK, length: int = 80, starts=None, n_starts: Optional[int] = None,
              first: int = 0, seed: int = 0, job_id: int = 0, p: float = 0.5, q: float = 2.0,

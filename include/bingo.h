@@ -154,6 +154,35 @@ int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uin
  * device address; make that first call before any stream capture. */
 int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs);
 
+/* ---- Batched programs -------------------------------------------------
+ * A program is an ordered list of walk-job sets and update batches executed
+ * with no host synchronisation between them (the reference runs the same
+ * sequence as separate synchronous calls, include/apps.cu:24-31). Each op
+ * sees the graph as left by the ops before it. All arrays must be device
+ * memory (starts may be NULL). With BINGO_RUN_GRAPH the program is captured
+ * once into a CUDA graph and replayed while its shape (op kinds, batch sizes,
+ * walk counts per job, array addresses) stays the same; walk-job contents
+ * (apps, lengths, seeds, p/q, stop probabilities) may change between
+ * replays. Update capacity is checked on the device: a batch that does not
+ * fit the graph arenas is not applied and the call returns
+ * BINGO_ERR_CAPACITY (the arenas are grown before the next call). */
+typedef enum bingo_op_kind { BINGO_OP_WALK = 0, BINGO_OP_INSERT = 1, BINGO_OP_DELETE = 2 } bingo_op_kind;
+
+typedef struct bingo_op {
+  int32_t kind;               /* bingo_op_kind */
+  uint32_t n_jobs;            /* WALK: jobs in this set, run as one persistent launch */
+  const bingo_walk_job* jobs; /* WALK */
+  const uint32_t* a;          /* INSERT: src   DELETE: vertex */
+  const uint32_t* b;          /* INSERT: dst   DELETE: slot */
+  const uint32_t* c;          /* INSERT: weight */
+  uint64_t k;                 /* INSERT / DELETE: batch size */
+  uint32_t* out_slots;        /* INSERT: slot ids (device, may be NULL) */
+} bingo_op;
+
+#define BINGO_RUN_GRAPH 1u
+
+int bingo_run(bingo_handle* h, const bingo_op* ops, uint32_t n_ops, uint32_t flags);
+
 /* Waits for all queued work; returns the first device-detected error since
  * the previous bingo_sync (or BINGO_OK). */
 int bingo_sync(bingo_handle* h);
