@@ -216,6 +216,131 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- batched (config 4)
+B_SCALE, B_PHASES, B_JOBS_PER_PHASE = 22, 16, 16
+B_SEED = 1234 + 4
+
+
+def make_batched_workload(steps_total: int):
+    """R-MAT scale 22, uniform [1, 65535] weights; 256 jobs (16 phases x 16)
+    with log-uniform start counts in [1K, 1M], lengths uniform in [5, 200],
+    apps uniform over {DeepWalk, node2vec with p, q in {0.25, 1, 4}, PPR
+    stop 0.15}; after each phase an update chunk of log-uniform [1K, 1M]
+    edges, half absent-pair inserts and half uniform deletes. Chunk sizes are
+    fixed across steps; their contents are fresh every step."""
+    from bingo_b200 import DEEPWALK, NODE2VEC, PPR, gen
+    n = 1 << B_SCALE
+    src, dst = gen.rmat(B_SCALE, EDGE_FACTOR, seed=B_SEED)
+    w = gen.weights(len(src), gen.W_UNIFORM, 1, 65535, seed=B_SEED + 1)
+    rng = np.random.default_rng(B_SEED + 2)
+    deg = np.bincount(src, minlength=n)
+    walkable = np.nonzero(deg)[0].astype(np.uint32)
+    pq = [(p_, q_) for p_ in (0.25, 1.0, 4.0) for q_ in (0.25, 1.0, 4.0)]
+    jobs = []
+    for j in range(B_PHASES * B_JOBS_PER_PHASE):
+        k = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        L = int(rng.integers(5, 201))
+        app = int(rng.integers(0, 3))
+        p_, q_ = pq[int(rng.integers(0, 9))]
+        jobs.append(dict(app=[DEEPWALK, NODE2VEC, PPR][app], length=L, starts=rng.choice(walkable, size=k),
+                         p=p_, q=q_, stop_prob=0.15, job_id=j))
+    chunk = [int(np.exp(rng.uniform(np.log(1e3), np.log(1e6)))) for _ in range(B_PHASES)]
+    ug = gen.UpdateGen(n, src, dst, seed=B_SEED + 3)
+    steps = []
+    for _ in range(steps_total):
+        ph = []
+        for c in chunk:
+            ph.append((ug.inserts(c // 2, gen.W_UNIFORM, 1, 65535), ug.deletes(c - c // 2)))
+        steps.append(ph)
+    return n, src, dst, w, jobs, chunk, steps
+
+
+def run_batched(args):
+    import torch
+    from bingo_b200 import Graph, WalkJob
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    total = args.warmup + args.steps
+    n, src, dst, w, jobs, chunk, steps = make_batched_workload(total)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)  # noqa: E731
+    starts = [t(j["starts"]) for j in jobs]
+    outs = [torch.empty((len(j["starts"]), j["length"]), dtype=torch.int32, device=dev) for j in jobs]
+    # fixed device batch buffers per chunk, refilled each step from per-step copies
+    buf = [((t(ins[0]), t(ins[1]), t(ins[2])), (t(de[0]), t(de[1]))) for ins, de in steps[0]]
+    per_step = [[((t(i[0]), t(i[1]), t(i[2])), (t(d[0]), t(d[1]))) for i, d in ph] for ph in steps]
+    slots = [torch.empty(len(steps[0][c][0][0]), dtype=torch.int32, device=dev) for c in range(B_PHASES)]
+
+    def walkjobs(phase, seed):
+        js = []
+        for j in range(phase * B_JOBS_PER_PHASE, (phase + 1) * B_JOBS_PER_PHASE):
+            J = jobs[j]
+            js.append(WalkJob(app=J["app"], length=J["length"], starts=starts[j], n_starts=len(J["starts"]),
+                              job_id=J["job_id"], seed=seed, p=J["p"], q=J["q"], stop_prob=J["stop_prob"],
+                              out=outs[j]))
+        return js
+
+    def refill(step):
+        for c in range(B_PHASES):
+            for dstb, srcb in zip(buf[c][0] + buf[c][1], per_step[step][c][0] + per_step[step][c][1]):
+                dstb.copy_(srcb, non_blocking=True)
+
+    def time_form(form):
+        g = Graph(device=local, synchronous=(form == "plain"))
+        g.set_stream(stream.cuda_stream)
+        g.load_edges(src, dst, w, n)
+        g.sync()
+        e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(total)]
+        steps0 = None
+        for i in range(total):
+            if i == args.warmup:
+                g.sync()
+                torch.cuda.synchronize(dev)
+                steps0 = g.stats()["walk_steps"]
+            e[i][0].record(stream)
+            refill(i)
+            if form == "plain":
+                for ph in range(B_PHASES):
+                    for job in walkjobs(ph, seed=1000 + i):
+                        g.walk_jobs([job], mode=1)
+                    (a, b, c), (du, ds) = buf[ph]
+                    g.insert_batch(a, b, c, out_slots=slots[ph])
+                    g.delete_batch(du, ds)
+            else:
+                ops = []
+                for ph in range(B_PHASES):
+                    (a, b, c), (du, ds) = buf[ph]
+                    ops += [("walk", walkjobs(ph, seed=1000 + i)), ("insert", a, b, c, slots[ph]), ("delete", du, ds)]
+                g.run(ops, graph=True)
+            e[i][1].record(stream)
+        g.sync()
+        torch.cuda.synchronize(dev)
+        wsteps = g.stats()["walk_steps"] - steps0
+        ms = sum(e[i][0].elapsed_time(e[i][1]) for i in range(args.warmup, total))
+        g.close()
+        upd = sum(chunk) * args.steps
+        return {"walk_steps_per_s": wsteps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                "edge_updates_per_s": upd / (ms / 1e3), "walk_steps_per_step": wsteps / args.steps}
+
+    plain = time_form("plain")
+    batched = time_form("batched")
+    if rank == 0:
+        line = {"metric": "walk_steps_per_s", "value": batched["walk_steps_per_s"], "unit": "steps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic",
+                "config": {"workload": "batched-rmat22", "scale": B_SCALE, "m": int(len(src)),
+                           "weights": "uniform[1,65535]", "jobs": len(jobs), "phases": B_PHASES,
+                           "walks_per_step": int(sum(len(j["starts"]) for j in jobs)),
+                           "update_edges_per_step": int(sum(chunk)),
+                           "form": "one CUDA graph per step: 16 x (16-job persistent walk launch, insert, delete)"},
+                "batched": batched, "plain": plain,
+                "batched_over_plain": batched["walk_steps_per_s"] / plain["walk_steps_per_s"]}
+        print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- reference CUDA build
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
@@ -506,6 +631,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+                    help="plain: BASELINE config 2 (default); batched: config 4, batched vs plain")
     ap.add_argument("--cpu-walks", type=int, default=131072)
     ap.add_argument("--ref-walks", type=int, default=131072)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
@@ -515,7 +642,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.impl == "reference":
+    if args.workload == "batched" and args.impl == "ours":
+        run_batched(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-cuda":
         run_reference_cuda(args)

@@ -37,9 +37,10 @@ struct __align__(32) AliasRec {
   uint32_t alt_base, alt_cnt;
 };
 
-struct __align__(8) HashEntry {
-  int32_t key;  // neighbour id or kEmptyKey
-  int32_t cnt;  // live multiplicity
+struct __align__(16) HashEntry {
+  int32_t key;                // neighbour id or kEmptyKey
+  int32_t cnt;                // live multiplicity
+  unsigned long long wsum;    // live weight sum of the edges to key
 };
 
 // ---------------------------------------------------------------------------

@@ -171,17 +171,22 @@ __global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint
 // Persistent walk kernel with per-lane refill. Each warp owns a range of
 // walk items and hands them to idle lanes; when the range runs out it pulls
 // the next kWalkChunk items from one device counter (reset by the host before
-// launch). APP >= 0: every item belongs to the single job J. APP < 0: items
-// index the concatenated jobs (prefix = running walk counts) and each lane
-// follows its own job's app.
+// launch). MULTI = false: every item is a walk of the single job J0.
+// MULTI = true: items index the concatenated jobs of a device job table
+// (prefix = running walk counts) and each lane follows its own job; APP >= 0
+// when every job of the table has that app, APP < 0 for a mixed table.
 constexpr uint32_t kWalkChunk = 32;
 static_assert(kBlock % 32 == 0, "whole warps");
 
 // Resident 256-thread blocks per SM each walk variant is compiled for
 // (register budget 65536 / (256 * blocks)): DeepWalk and sampling 32
-// registers, PPR 40, node2vec 48, the mixed-job kernel 64.
-constexpr int walk_min_blocks(int app) {
-  return app == APP_DEEPWALK || app == APP_SAMPLING ? 8 : app == APP_PPR ? 6 : app == APP_NODE2VEC ? 5 : 4;
+// registers; PPR 40 (48 with a job table); node2vec 48 (64 with a job
+// table); the mixed-app kernel 64.
+constexpr int walk_min_blocks(int app, bool multi) {
+  return app == APP_DEEPWALK || app == APP_SAMPLING ? 8
+         : app == APP_PPR                           ? (multi ? 5 : 6)
+         : app == APP_NODE2VEC                      ? (multi ? 4 : 5)
+                                                    : 4;
 }
 
 __device__ __forceinline__ bool begin_any(const WalkView& W, const WalkJobDev& J, uint32_t i, LaneWalk& s,
@@ -202,10 +207,10 @@ __device__ __forceinline__ bool advance_any(const WalkView& W, const WalkJobDev&
   }
 }
 
-template <int APP>
-__global__ void __launch_bounds__(kBlock, walk_min_blocks(APP)) k_walk(WalkView W, WalkJobDev J0, const WalkJobDev* __restrict__ jobs,
-                                                 const uint32_t* __restrict__ prefix, uint32_t n_jobs, uint32_t total,
-                                                 uint32_t* queue) {
+template <int APP, bool MULTI>
+__global__ void __launch_bounds__(kBlock, walk_min_blocks(APP, MULTI))
+    k_walk(WalkView W, WalkJobDev J0, const WalkJobDev* __restrict__ jobs, const uint32_t* __restrict__ prefix,
+           uint32_t n_jobs, uint32_t total, uint32_t* queue) {
   __shared__ __align__(16) int32_t obuf[kBlock][8];
   const int lane = threadIdx.x & 31;
   LaneWalk s;
@@ -230,7 +235,7 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP)) k_walk(WalkView 
       const uint32_t rank = __popc(idle & lanemask_lt());
       if (!active && rank < take) {
         const uint32_t item = wb + rank;
-        if (APP >= 0) {
+        if (!MULTI) {
           active = walk_begin<APP>(W, J0, item, s, o, obuf, moves);
         } else {
           uint32_t lo = 0, hi = n_jobs;
@@ -242,7 +247,10 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP)) k_walk(WalkView 
               hi = mid;
           }
           jid = lo;
-          active = begin_any(W, jobs[lo], item - prefix[lo], s, o, obuf, moves);
+          if (APP >= 0)
+            active = walk_begin<APP>(W, jobs[lo], item - prefix[lo], s, o, obuf, moves);
+          else
+            active = begin_any(W, jobs[lo], item - prefix[lo], s, o, obuf, moves);
         }
       }
       wb += take;
@@ -250,8 +258,11 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP)) k_walk(WalkView 
     }
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      if (APP >= 0)
-        active = walk_advance<APP == APP_SAMPLING ? APP_DEEPWALK : APP>(W, J0, s, o, obuf, moves);
+      constexpr int A = APP == APP_SAMPLING ? APP_DEEPWALK : APP;
+      if (!MULTI)
+        active = walk_advance<A>(W, J0, s, o, obuf, moves);
+      else if (APP >= 0)
+        active = walk_advance<A>(W, jobs[jid], s, o, obuf, moves);
       else
         active = advance_any(W, jobs[jid], s, o, obuf, moves);
     }
@@ -270,18 +281,124 @@ __global__ void k_philox(const uint32_t* ctr, unsigned long long count, uint32_t
   }
 }
 
-// Resident 256-thread blocks per SM of walk kernel k_walk<APP> (register-limited):
-// the persistent grid is exactly one full wave.
-template <int APP>
+// Resident 256-thread blocks per SM of walk kernel k_walk<APP, MULTI>
+// (register-limited): the persistent grid is exactly one full wave.
+template <int APP, bool MULTI>
 unsigned walk_blocks_per_sm() {
   static int b = 0;
   if (!b) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<APP>, kBlock, 0) != cudaSuccess || b <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<APP, MULTI>, kBlock, 0) != cudaSuccess || b <= 0) {
       cudaGetLastError();
       b = 4;
     }
   }
   return (unsigned)b;
+}
+
+// Launches the persistent walk kernel for a device job table whose jobs all
+// have app `app` (or any app when app < 0).
+void launch_walk_table(cudaStream_t st, int app, const WalkView& W, const WalkJobDev& J0, const WalkJobDev* jobs,
+                       const uint32_t* prefix, uint32_t n_jobs, uint32_t total, uint32_t* queue) {
+  switch (app) {
+    case APP_DEEPWALK:
+      k_walk<APP_DEEPWALK, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_DEEPWALK, true>()), kBlock, 0,
+                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      break;
+    case APP_NODE2VEC:
+      k_walk<APP_NODE2VEC, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_NODE2VEC, true>()), kBlock, 0,
+                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      break;
+    case APP_PPR:
+      k_walk<APP_PPR, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_PPR, true>()), kBlock, 0, st>>>(
+          W, J0, jobs, prefix, n_jobs, total, queue);
+      break;
+    case APP_SAMPLING:
+      k_walk<APP_SAMPLING, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_SAMPLING, true>()), kBlock, 0,
+                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      break;
+    default:
+      k_walk<-1, true><<<grid_for(total, kBlock, walk_blocks_per_sm<-1, true>()), kBlock, 0, st>>>(
+          W, J0, jobs, prefix, n_jobs, total, queue);
+      break;
+  }
+  cuda_check(cudaGetLastError(), "walk launch");
+}
+
+// A job table for one persistent launch: jobs of one app (or all apps).
+struct WalkGroup {
+  int app;            // app of every job, or -1 for a mixed table
+  size_t job_off;     // first job in the concatenated table
+  size_t pf_off;      // first prefix entry (n_jobs + 1 entries)
+  uint32_t n_jobs;
+  uint32_t total;     // walks
+};
+
+bool walk_split_by_app() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("BINGO_WALK_SPLIT");
+    v = (e && std::strcmp(e, "1") == 0) ? 1 : 0;  // one mixed launch measured faster
+  }
+  return v == 1;
+}
+
+double walk_cost(const WalkJobDev& J);
+
+// Appends the jobs `in` to (table, prefix) as one group per app present
+// (or one mixed group), each ordered by expected walk cost, most expensive
+// first, so the longest walks start earliest. Outputs are per job, so the
+// order does not change any result.
+void build_walk_groups(const WalkJobDev* in, uint32_t n, bool split, std::vector<WalkJobDev>& table,
+                       std::vector<uint32_t>& prefix, std::vector<WalkGroup>& groups) {
+  std::vector<uint32_t> idx;
+  for (int app = split ? 0 : -1; app <= (split ? 3 : -1); ++app) {
+    idx.clear();
+    for (uint32_t j = 0; j < n; ++j)
+      if ((app < 0 || in[j].app == app) && in[j].n) idx.push_back(j);
+    if (idx.empty()) continue;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](uint32_t a, uint32_t b) { return walk_cost(in[a]) > walk_cost(in[b]); });
+    WalkGroup g{app, table.size(), prefix.size(), (uint32_t)idx.size(), 0};
+    uint64_t t = 0;
+    prefix.push_back(0);
+    for (uint32_t j : idx) {
+      table.push_back(in[j]);
+      t += in[j].n;
+      prefix.push_back((uint32_t)t);
+    }
+    g.total = (uint32_t)t;
+    groups.push_back(g);
+  }
+}
+
+// Expected relative cost of one walk of a job, used to hand out the most
+// expensive walks first (shorter tails in persistent launches).
+double walk_cost(const WalkJobDev& J) {
+  if (J.app == APP_SAMPLING) return 1.0;
+  double L = J.L;
+  if (J.app == APP_PPR) {
+    const double stop = (double)J.thr_stop / 4294967296.0;
+    const double geo = stop > 0 ? 1.0 / stop : 1e9;
+    L = (J.flags & kWalkPprTail) ? geo : std::min(L, geo);
+  }
+  if (J.app == APP_NODE2VEC) L *= 3.0;
+  return L;
+}
+
+uint64_t prob_threshold(double p);
+
+// node2vec weights 1/p (return), 1 (neighbour of the previous vertex), 1/q
+// (other); acceptance against the envelope max(1, 1/q); a larger 1/p is
+// handled by the return region (ret_excess). PPR stop threshold.
+void set_thresholds(WalkJobDev& D, const bingo_walk_job& J) {
+  const bool n2v = J.app == BINGO_NODE2VEC;
+  const double wr = n2v ? 1.0 / J.p : 1.0, wo = n2v ? 1.0 / J.q : 1.0;
+  const double am = std::max(1.0, wo), rr = wr / am;
+  D.thr_ret = prob_threshold(rr);
+  D.ret_excess = rr > 1.0 ? rr - 1.0 : 0.0;
+  D.thr_in = prob_threshold(1.0 / am);
+  D.thr_out = prob_threshold(wo / am);
+  D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
 }
 
 uint64_t prob_threshold(double p) {
@@ -777,12 +894,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     D.k1 = (uint32_t)(J.seed >> 32);
     D.flags = J.flags;
     D.pad = 0;
-    const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
-    const double wmax = std::max(wr, std::max(1.0, wo));
-    D.thr_ret = prob_threshold(wr / wmax);
-    D.thr_in = prob_threshold(1.0 / wmax);
-    D.thr_out = prob_threshold(wo / wmax);
-    D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+    set_thresholds(D, J);
     D.starts = J.starts;
     if (s_off[j] != ~0ull) {
       uint32_t* d = wstart_.as<uint32_t>() + s_off[j];
@@ -810,7 +922,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq), "walk launch");
     ++launches_;
   };
-  queue_.ensure(4 * std::max<uint32_t>(n_jobs, 1), "walk queue");
+  queue_.ensure(4 * std::max<uint32_t>(n_jobs, 4), "walk queue");
   uint32_t* q = queue_.as<uint32_t>();
   if (mode == BINGO_WALK_PLAIN) {
     // One launch per job, each with its own work counter.
@@ -820,34 +932,42 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
       const uint32_t nw = (uint32_t)dj[j].n;
       switch (dj[j].app) {
         case APP_DEEPWALK:
-          launch(k_walk<APP_DEEPWALK>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK>()), dj[j], nullptr,
+          launch(k_walk<APP_DEEPWALK, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK, false>()), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
         case APP_NODE2VEC:
-          launch(k_walk<APP_NODE2VEC>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC>()), dj[j], nullptr,
+          launch(k_walk<APP_NODE2VEC, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC, false>()), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
         case APP_PPR:
-          launch(k_walk<APP_PPR>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR>()), dj[j], nullptr, nullptr, 0,
+          launch(k_walk<APP_PPR, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR, false>()), dj[j], nullptr, nullptr, 0,
                  nw, q + j);
           break;
         default:
-          launch(k_walk<APP_SAMPLING>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING>()), dj[j], nullptr,
+          launch(k_walk<APP_SAMPLING, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING, false>()), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
       }
     }
   } else if (prefix[n_jobs]) {
-    jobs_.ensure(n_jobs * sizeof(WalkJobDev), "walk jobs");
-    prefix_.ensure((n_jobs + 1) * 4, "walk jobs");
-    std::vector<uint32_t> p32(prefix.begin(), prefix.end());
-    cuda_check(cudaMemcpyAsync(jobs_.p, dj.data(), n_jobs * sizeof(WalkJobDev), cudaMemcpyHostToDevice, stream_),
+    // One persistent launch per app present (or one mixed launch).
+    std::vector<WalkJobDev> table;
+    std::vector<uint32_t> pf;
+    std::vector<WalkGroup> groups;
+    build_walk_groups(dj.data(), n_jobs, walk_split_by_app(), table, pf, groups);
+    jobs_.ensure(table.size() * sizeof(WalkJobDev), "walk jobs");
+    prefix_.ensure(pf.size() * 4, "walk jobs");
+    cuda_check(cudaMemcpyAsync(jobs_.p, table.data(), table.size() * sizeof(WalkJobDev), cudaMemcpyHostToDevice,
+                               stream_),
                "jobs H2D");
-    cuda_check(cudaMemcpyAsync(prefix_.p, p32.data(), (n_jobs + 1) * 4, cudaMemcpyHostToDevice, stream_),
-               "prefix H2D");
-    cuda_check(cudaMemsetAsync(q, 0, 4, stream_), "queue reset");
-    launch(k_walk<-1>, grid_for(prefix[n_jobs], kBlock, walk_blocks_per_sm<-1>()), dj[0],
-           jobs_.as<WalkJobDev>(), prefix_.as<uint32_t>(), n_jobs, (uint32_t)prefix[n_jobs], q);
+    cuda_check(cudaMemcpyAsync(prefix_.p, pf.data(), pf.size() * 4, cudaMemcpyHostToDevice, stream_), "prefix H2D");
+    cuda_check(cudaMemsetAsync(q, 0, 4 * groups.size(), stream_), "queue reset");
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      const WalkGroup& G = groups[gi];
+      launch_walk_table(stream_, G.app, W, table[G.job_off], jobs_.as<WalkJobDev>() + G.job_off,
+                        prefix_.as<uint32_t>() + G.pf_off, G.n_jobs, G.total, q + gi);
+      ++launches_;
+    }
   }
   for (uint32_t j = 0; j < n_jobs; ++j)
     if (o_off[j] != ~0ull) {
@@ -972,17 +1092,17 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
   if (kmax) ensure_batch_scratch(kmax);
   ensure_headroom(k_ins);
   mix(arena_gen_), mix(n_);
-  std::vector<WalkJobDev> dj;
+  std::vector<WalkJobDev> dj, table;
   std::vector<uint32_t> pf;
-  std::vector<uint64_t> job_off(n_ops, 0), pf_off(n_ops, 0), totals(n_ops, 0);
+  std::vector<WalkGroup> groups;
+  std::vector<size_t> grp_begin(n_ops, 0), grp_end(n_ops, 0);
+  const bool split = walk_split_by_app();
   dj.reserve(n_jobs_total);
   for (uint32_t i = 0; i < n_ops; ++i) {
     const bingo_op& o = ops[i];
     if (o.kind != BINGO_OP_WALK) continue;
-    job_off[i] = dj.size();
-    pf_off[i] = pf.size();
+    dj.clear();
     uint64_t t = 0;
-    pf.push_back(0);
     for (uint32_t j = 0; j < o.n_jobs; ++j) {
       const bingo_walk_job& J = o.jobs[j];
       if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
@@ -1002,7 +1122,7 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
       }
       t += J.n_starts;
       if (t >= (1ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one op");
-      pf.push_back((uint32_t)t);
+      if (split) mix((uint64_t)J.app);
       WalkJobDev D;
       D.app = J.app;
       D.L = J.length;
@@ -1014,35 +1134,33 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
       D.k1 = (uint32_t)(J.seed >> 32);
       D.flags = J.flags;
       D.pad = 0;
-      const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
-      const double wmax = std::max(wr, std::max(1.0, wo));
-      D.thr_ret = prob_threshold(wr / wmax);
-      D.thr_in = prob_threshold(1.0 / wmax);
-      D.thr_out = prob_threshold(wo / wmax);
-      D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+      set_thresholds(D, J);
       D.out = J.out;
       dj.push_back(D);
     }
-    totals[i] = t;
+    grp_begin[i] = groups.size();
+    build_walk_groups(dj.data(), (uint32_t)dj.size(), split, table, pf, groups);
+    grp_end[i] = groups.size();
   }
   // Job tables are read by the walk kernels from device memory, so their
   // contents may change between replays of a captured program.
-  if (!dj.empty()) {
-    const size_t jb = dj.size() * sizeof(WalkJobDev), pb = pf.size() * 4;
-    if (jb > prog_jobs_.bytes || pb > prog_prefix_.bytes || n_walk_ops * 4 > prog_queue_.bytes) drop_graph();
+  if (!table.empty()) {
+    const size_t jb = table.size() * sizeof(WalkJobDev), pb = pf.size() * 4, qb = groups.size() * 4;
+    if (jb > prog_jobs_.bytes || pb > prog_prefix_.bytes || qb > prog_queue_.bytes) drop_graph();
     prog_jobs_.ensure(jb, "program jobs");
     prog_prefix_.ensure(pb, "program jobs");
-    prog_queue_.ensure(std::max<uint64_t>(n_walk_ops, 1) * 4, "program queue");
-    cuda_check(cudaMemcpyAsync(prog_jobs_.p, dj.data(), jb, cudaMemcpyHostToDevice, stream_), "program jobs H2D");
+    prog_queue_.ensure(std::max<size_t>(qb, 4), "program queue");
+    cuda_check(cudaMemcpyAsync(prog_jobs_.p, table.data(), jb, cudaMemcpyHostToDevice, stream_), "program jobs H2D");
     cuda_check(cudaMemcpyAsync(prog_prefix_.p, pf.data(), pb, cudaMemcpyHostToDevice, stream_), "program jobs H2D");
   }
+  (void)n_walk_ops;
   mix((uint64_t)(uintptr_t)prog_jobs_.p), mix((uint64_t)(uintptr_t)ctl_.p), mix((uint64_t)(uintptr_t)cub_tmp_.p);
   mix(cub_tmp_.bytes);
 
   const uint64_t launches0 = launches_;
   auto enqueue_all = [&]() {
-    if (n_walk_ops) cuda_check(cudaMemsetAsync(prog_queue_.p, 0, n_walk_ops * 4, stream_), "program queue reset");
-    uint32_t wi = 0;
+    if (!groups.empty())
+      cuda_check(cudaMemsetAsync(prog_queue_.p, 0, groups.size() * 4, stream_), "program queue reset");
     const WalkView W = wview();
     for (uint32_t i = 0; i < n_ops; ++i) {
       const bingo_op& o = ops[i];
@@ -1051,14 +1169,13 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
       } else if (o.kind == BINGO_OP_DELETE && o.k) {
         enqueue_delete(o.a, o.b, o.k);
       } else if (o.kind == BINGO_OP_WALK) {
-        uint32_t* q = prog_queue_.as<uint32_t>() + wi++;
-        if (!totals[i]) continue;
-        WalkJobDev* jt = prog_jobs_.as<WalkJobDev>() + job_off[i];
-        const uint32_t* pp = prog_prefix_.as<uint32_t>() + pf_off[i];
-        k_walk<-1><<<grid_for(totals[i], kBlock, walk_blocks_per_sm<-1>()), kBlock, 0, stream_>>>(
-            W, dj[job_off[i]], jt, pp, o.n_jobs, (uint32_t)totals[i], q);
-        cuda_check(cudaGetLastError(), "program walk launch");
-        ++launches_;
+        for (size_t gi = grp_begin[i]; gi < grp_end[i]; ++gi) {
+          const WalkGroup& G = groups[gi];
+          launch_walk_table(stream_, G.app, W, table[G.job_off], prog_jobs_.as<WalkJobDev>() + G.job_off,
+                            prog_prefix_.as<uint32_t>() + G.pf_off, G.n_jobs, G.total,
+                            prog_queue_.as<uint32_t>() + gi);
+          ++launches_;
+        }
       }
     }
   };
@@ -1169,12 +1286,7 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
     D.k1 = (uint32_t)(J.seed >> 32);
     D.flags = J.flags;
     D.pad = 0;
-    const double wr = J.app == BINGO_NODE2VEC ? 1.0 / J.p : 1.0, wo = J.app == BINGO_NODE2VEC ? 1.0 / J.q : 1.0;
-    const double wmax = std::max(wr, std::max(1.0, wo));
-    D.thr_ret = prob_threshold(wr / wmax);
-    D.thr_in = prob_threshold(1.0 / wmax);
-    D.thr_out = prob_threshold(wo / wmax);
-    D.thr_stop = prob_threshold(J.app == BINGO_PPR ? J.stop_prob : 0.0);
+    set_thresholds(D, J);
     D.out = J.out;
   }
   if (!total) return;
@@ -1186,7 +1298,7 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
              "no-alloc prefix H2D");
   cuda_check(cudaMemsetAsync(&scratch->queue, 0, 4, stream_), "no-alloc counter reset");
   const WalkView W = wview();
-  k_walk<-1><<<grid_for(total, kBlock, walk_blocks_per_sm<-1>()), kBlock, 0, stream_>>>(
+  k_walk<-1, true><<<grid_for(total, kBlock, walk_blocks_per_sm<-1, true>()), kBlock, 0, stream_>>>(
       W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue);
   cuda_check(cudaGetLastError(), "no-alloc walk launch");
   ++launches_;

@@ -59,13 +59,15 @@ __device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uin
 }
 
 // ---------------------------------------------------------------------------
-// Adjacency index (node2vec neighbour test), linear probing on mix32.
-__device__ __forceinline__ void hash_add(HashEntry* tab, uint32_t hmask, uint32_t v, uint32_t* claimed) {
+// Adjacency index (node2vec), linear probing on mix32: per neighbour the
+// live edge count and live weight sum.
+__device__ __forceinline__ void hash_add(HashEntry* tab, uint32_t hmask, uint32_t v, uint32_t w, uint32_t* claimed) {
   uint32_t h = mix32(v) & hmask;
   for (uint32_t probe = 0; probe <= hmask; ++probe) {
     const int prev = atomicCAS(&tab[h].key, kEmptyKey, (int)v);
     if (prev == kEmptyKey || prev == (int)v) {
       atomicAdd(&tab[h].cnt, 1);
+      atomicAdd(&tab[h].wsum, (unsigned long long)w);
       if (prev == kEmptyKey) ++*claimed;
       return;
     }
@@ -73,12 +75,13 @@ __device__ __forceinline__ void hash_add(HashEntry* tab, uint32_t hmask, uint32_
   }
 }
 
-__device__ __forceinline__ void hash_sub(HashEntry* tab, uint32_t hmask, uint32_t v) {
+__device__ __forceinline__ void hash_sub(HashEntry* tab, uint32_t hmask, uint32_t v, uint32_t w) {
   uint32_t h = mix32(v) & hmask;
   for (uint32_t probe = 0; probe <= hmask; ++probe) {
     const int k = tab[h].key;
     if (k == (int)v) {
       atomicSub(&tab[h].cnt, 1);
+      atomicAdd(&tab[h].wsum, 0ull - (unsigned long long)w);
       return;
     }
     if (k == kEmptyKey) return;
@@ -86,15 +89,27 @@ __device__ __forceinline__ void hash_sub(HashEntry* tab, uint32_t hmask, uint32_
   }
 }
 
-__device__ __forceinline__ bool hash_has(const HashEntry* tab, uint32_t hmask, uint32_t v) {
+// Index of v's entry, or -1.
+__device__ __forceinline__ int hash_find(const HashEntry* tab, uint32_t hmask, uint32_t v) {
   uint32_t h = mix32(v) & hmask;
   for (uint32_t probe = 0; probe <= hmask; ++probe) {
-    const HashEntry e = tab[h];
-    if (e.key == (int)v) return e.cnt > 0;
-    if (e.key == kEmptyKey) return false;
+    const int k = __ldg(&tab[h].key);
+    if (k == (int)v) return (int)h;
+    if (k == kEmptyKey) return -1;
     h = (h + 1) & hmask;
   }
-  return false;
+  return -1;
+}
+
+__device__ __forceinline__ bool hash_has(const HashEntry* tab, uint32_t hmask, uint32_t v) {
+  const int h = hash_find(tab, hmask, v);
+  return h >= 0 && __ldg(&tab[h].cnt) > 0;
+}
+
+// Live weight sum of the edges to v (0 when there are none).
+__device__ __forceinline__ unsigned long long hash_weight(const HashEntry* tab, uint32_t hmask, uint32_t v) {
+  const int h = hash_find(tab, hmask, v);
+  return h >= 0 && __ldg(&tab[h].cnt) > 0 ? __ldg(&tab[h].wsum) : 0ull;
 }
 
 // ---------------------------------------------------------------------------
@@ -255,18 +270,18 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
     if (P.new_hcap) {
       // Rebuild from every live slot into a fresh table.
       HashEntry* tab = S.hash + res[A_HASH];
-      for (uint32_t i = lane; i < P.new_hcap; i += 32) tab[i] = HashEntry{kEmptyKey, 0};
+      for (uint32_t i = lane; i < P.new_hcap; i += 32) tab[i] = HashEntry{kEmptyKey, 0, 0ull};
       __syncwarp();
       for (uint32_t i = lane; i < M.ecnt; i += 32) {
         const EdgeRec e = S.edges[M.eoff + i];
-        if (e.w) hash_add(tab, P.new_hcap - 1, e.v, &claimed);
+        if (e.w) hash_add(tab, P.new_hcap - 1, e.v, e.w, &claimed);
       }
       R.hoff = (uint32_t)res[A_HASH];
       R.hmask = P.new_hcap - 1;
       M.hcap = P.new_hcap;
       M.hkeys = warp_sum_u32(claimed);
     } else {
-      for (uint32_t i = lane; i < len; i += 32) hash_add(S.hash + R.hoff, R.hmask, seg_v[i], &claimed);
+      for (uint32_t i = lane; i < len; i += 32) hash_add(S.hash + R.hoff, R.hmask, seg_v[i], seg_w[i], &claimed);
       M.hkeys += warp_sum_u32(claimed);
     }
   }
@@ -354,7 +369,7 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
     __syncwarp();
     if (valid) {
       S.edges[M.eoff + slot].w = 0u;
-      if (S.node2vec && R.hmask) hash_sub(S.hash + R.hoff, R.hmask, e.v);
+      if (S.node2vec && R.hmask) hash_sub(S.hash + R.hoff, R.hmask, e.v, e.w);
     }
     M.live -= __popc(vmask);
     __syncwarp();

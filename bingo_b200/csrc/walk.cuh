@@ -30,8 +30,18 @@ struct WalkJobDev {
   uint32_t flags;
   uint32_t pad;
   unsigned long long thr_ret, thr_in, thr_out, thr_stop;  // 33-bit acceptance thresholds
+  double ret_excess;  // node2vec: (1/p) / max(1, 1/q) - 1 when positive, else 0
   int32_t* out;
 };
+
+// p in [0, 1] -> 33-bit threshold floor(p * 2^32) (2^32 = always); the same
+// formula as the host side, with IEEE-rounded operations.
+__device__ __forceinline__ unsigned long long prob_threshold_dev(double p) {
+  if (!(p > 0.0)) return 0ull;
+  if (p >= 1.0) return 1ull << 32;
+  const double t = floor(__dmul_rn(p, 4294967296.0));
+  return t >= 4294967296.0 ? (1ull << 32) : (unsigned long long)t;
+}
 
 struct WalkView {
   uint32_t n;
@@ -64,81 +74,17 @@ __device__ __forceinline__ bool adjacent(const WalkView& W, const VertexRec& Rpr
   return hash_has(W.hash + Rprev.hoff, Rprev.hmask, x);
 }
 
-// Runs walk `i` of job J to completion, writing its row. Returns the number
-// of moves made (the produced steps).
-template <int APP>
-__device__ __forceinline__ uint32_t run_walk(const WalkView& W, const WalkJobDev& J, uint32_t i) {
-  const uint32_t start = J.starts ? J.starts[i] : J.first + i;
-  if (APP == APP_SAMPLING) {
-    int32_t x = -1;
-    if (start < W.n) {
-      const VertexRec R = load_vrec(W, start);
-      if (R.m) x = (int32_t)sample_at(W, R, philox(i, 1, 0, J.job, J.k0, J.k1));
-    } else {
-      set_err(W.err, E_RANGE);
-    }
-    J.out[i] = x;
-    return x >= 0;
-  }
-  const uint32_t L = J.L;
-  int32_t* row = J.out + (size_t)i * L;
-  if (L == 0) return 0;
-  if (start >= W.n) {
-    set_err(W.err, E_RANGE);
-    for (uint32_t j = 0; j < L; ++j) row[j] = -1;
-    return 0;
-  }
-  row[0] = (int32_t)start;
-  uint32_t cur = start, pos = 0, moves = 0;
-  int64_t prev = -1;
-  VertexRec Rprev{0, 0, 0, 0};
-  const bool tail = APP == APP_PPR && (J.flags & kWalkPprTail);
-  for (uint32_t j = 1;; ++j) {
-    if (j >= L && !tail) break;
-    if (tail && j >= kMaxPprSteps) break;
-    pos = j < L ? j : L - 1;
-    const VertexRec R = load_vrec(W, cur);
-    if (!R.m) {
-      row[pos] = -1;
-      break;
-    }
-    uint32_t x;
-    if (APP == APP_NODE2VEC && prev >= 0) {
-      for (uint32_t t = 0;; ++t) {
-        x = sample_at(W, R, philox(i, j, 2 * t, J.job, J.k0, J.k1));
-        const unsigned long long thr =
-            (int64_t)x == prev ? J.thr_ret : (adjacent(W, Rprev, x) ? J.thr_in : J.thr_out);
-        const uint32_t a = philox(i, j, 2 * t + 1, J.job, J.k0, J.k1).x;
-        if ((unsigned long long)a < thr || t + 1 == kMaxNode2vecTrials) break;
-      }
-    } else {
-      x = sample_at(W, R, philox(i, j, 0, J.job, J.k0, J.k1));
-    }
-    row[pos] = (int32_t)x;
-    ++moves;
-    prev = cur;
-    Rprev = R;
-    cur = x;
-    if (APP == APP_PPR && (unsigned long long)philox(i, j, 1, J.job, J.k0, J.k1).x < J.thr_stop) break;
-  }
-  for (uint32_t j = pos + 1; j < L; ++j) row[j] = -1;
-  return moves;
-}
-
-__device__ __forceinline__ uint32_t run_walk_any(const WalkView& W, const WalkJobDev& J, uint32_t i) {
-  switch (J.app) {
-    case APP_DEEPWALK: return run_walk<APP_DEEPWALK>(W, J, i);
-    case APP_NODE2VEC: return run_walk<APP_NODE2VEC>(W, J, i);
-    case APP_PPR: return run_walk<APP_PPR>(W, J, i);
-    default: return run_walk<APP_SAMPLING>(W, J, i);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// Step-at-a-time form for the persistent kernels: a lane advances its walk
+// Step-at-a-time walks for the persistent kernels: a lane advances its walk
 // one step per iteration and pulls a new walk as soon as its walk ends, so
-// dead-ended and early-stopped walks do not idle their warp. Same counters,
-// same outputs as run_walk.
+// dead-ended and early-stopped walks do not idle their warp.
+//
+// Counters: step j of walk i in job `job` draws Philox block
+// (i, j, trial, job) under key seed. DeepWalk uses trial 0; PPR samples with
+// trial 0 and tests its stop with trial 1; node2vec proposes with trial 2t
+// and accepts with trial 2t + 1 (t = 0, 1, ...; the first step is
+// first-order and takes trial 0). Row position j holds the j-th move; a walk
+// that reaches a vertex without out-edges writes -1 there and pads the rest.
 //
 // Row output goes through an 8-entry (one 32-byte sector) staging buffer per
 // lane in shared memory: a lane writes its row a whole sector at a time with
@@ -262,12 +208,38 @@ __device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev
   } else {
     uint32_t x;
     if (APP == APP_NODE2VEC && s.prev >= 0) {
+      // Return region: when 1/p exceeds the envelope max(1, 1/q), the excess
+      // mass (ret_excess x w(cur -> prev)) returns to prev directly, with
+      // probability D / (T + D) per trial (word y of the acceptance block).
+      unsigned long long region = 0;
+      if (J.ret_excess > 0.0) {
+        const unsigned long long wp = hash_weight(W.hash + R.hoff, R.hmask, (uint32_t)s.prev);
+        if (wp) {
+          const double T = (double)__ldg(&W.alias[R.aoff].T);
+          const double D = __dmul_rn(J.ret_excess, (double)wp);
+          region = prob_threshold_dev(__ddiv_rn(D, __dadd_rn(T, D)));
+        }
+      }
+      // Otherwise accept a proposal x with probability weight(class(x)) /
+      // envelope. The adjacency probe is skipped when the acceptance draw is
+      // below both the in- and out-class thresholds (the outcome is then the
+      // same for every class x can be in).
+      const unsigned long long io_min = J.thr_in < J.thr_out ? J.thr_in : J.thr_out;
       for (uint32_t t = 0;; ++t) {
+        const Rand4 a = philox(s.i, s.j, 2 * t + 1, J.job, J.k0, J.k1);
+        if ((unsigned long long)a.y < region) {
+          x = (uint32_t)s.prev;
+          break;
+        }
         x = sample_at(W, R, philox(s.i, s.j, 2 * t, J.job, J.k0, J.k1));
-        const unsigned long long thr =
-            (int32_t)x == s.prev ? J.thr_ret : (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
-        const uint32_t a = philox(s.i, s.j, 2 * t + 1, J.job, J.k0, J.k1).x;
-        if ((unsigned long long)a < thr || t + 1 == kMaxNode2vecTrials) break;
+        bool ok;
+        if ((int32_t)x == s.prev)
+          ok = a.x < J.thr_ret;
+        else if (a.x < io_min)
+          ok = true;
+        else
+          ok = a.x < (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
+        if (ok || t + 1 == kMaxNode2vecTrials) break;
       }
     } else {
       x = sample_at(W, R, philox(s.i, s.j, 0, J.job, J.k0, J.k1));

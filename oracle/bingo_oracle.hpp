@@ -144,19 +144,36 @@ inline uint64_t prob_threshold(double p) {
   return t >= 4294967296.0 ? (1ull << 32) : (uint64_t)t;
 }
 
+// node2vec weights: 1/p for returning to the previous vertex, 1 for a
+// neighbour of it, 1/q otherwise. Proposals are accepted against the envelope
+// am = max(1, 1/q); when 1/p exceeds it, the excess mass (1/p / am - 1) x
+// w(cur -> prev) becomes a separate region that returns to the previous
+// vertex directly (the "outlier" treatment of KnightKing, Yang et al.,
+// SOSP'19), so a large 1/p does not inflate the rejection rate.
 struct WalkThresholds {
   uint64_t ret, in, out, stop;
+  double ret_excess;  // 0 when 1/p fits under the envelope
 };
 
 inline WalkThresholds walk_thresholds(double p, double q, double stop) {
   WalkThresholds t{};
   const double wr = 1.0 / p, wi = 1.0, wo = 1.0 / q;
-  const double wmax = std::max(wr, std::max(wi, wo));
-  t.ret = prob_threshold(wr / wmax);
-  t.in = prob_threshold(wi / wmax);
-  t.out = prob_threshold(wo / wmax);
+  const double am = std::max(wi, wo);
+  const double rr = wr / am;
+  t.ret = prob_threshold(rr);
+  t.ret_excess = rr > 1.0 ? rr - 1.0 : 0.0;
+  t.in = prob_threshold(wi / am);
+  t.out = prob_threshold(wo / am);
   t.stop = prob_threshold(stop);
   return t;
+}
+
+// Probability threshold of the return region at a step: D / (T + D) with
+// D = excess x w(cur -> prev), T = total live weight at cur.
+inline uint64_t region_threshold(double excess, uint64_t wp, uint64_t T) {
+  if (!(excess > 0.0) || !wp) return 0;
+  const double D = excess * (double)wp;
+  return prob_threshold(D / ((double)T + D));
 }
 
 // ---------------------------------------------------------------------------
@@ -174,7 +191,7 @@ struct ExactGraph {
     uint32_t live = 0;
     int m = 0;
     AliasSlot alias[32];
-    std::unordered_map<uint32_t, uint32_t> adj;  // node2vec adjacency: neighbour -> live multiplicity
+    std::unordered_map<uint32_t, std::pair<uint32_t, uint64_t>> adj;  // neighbour -> (live multiplicity, weight sum)
     Vertex() { std::memset(gi, -1, sizeof gi); }
     Group& grp(int k) {
       if (gi[k] < 0) {
@@ -194,14 +211,24 @@ struct ExactGraph {
 
   static inline uint32_t rank_of(uint32_t w, int k) { return __builtin_popcount(w & ((1u << k) - 1u)); }
 
-  static void adj_add(Vertex& X, uint32_t v) { ++X.adj[v]; }
-  static void adj_sub(Vertex& X, uint32_t v) {
+  static void adj_add(Vertex& X, uint32_t v, uint32_t w) {
+    auto& e = X.adj[v];
+    ++e.first;
+    e.second += w;
+  }
+  static void adj_sub(Vertex& X, uint32_t v, uint32_t w) {
     auto it = X.adj.find(v);
-    if (it != X.adj.end() && it->second && --it->second == 0) X.adj.erase(it);
+    if (it == X.adj.end() || !it->second.first) return;
+    it->second.second -= w;
+    if (--it->second.first == 0) X.adj.erase(it);
   }
   static bool adj_has(const Vertex& X, uint32_t v) {
     auto it = X.adj.find(v);
-    return it != X.adj.end() && it->second > 0;
+    return it != X.adj.end() && it->second.first > 0;
+  }
+  static uint64_t adj_weight(const Vertex& X, uint32_t v) {
+    auto it = X.adj.find(v);
+    return it != X.adj.end() && it->second.first > 0 ? it->second.second : 0;
   }
 
   // Append one edge to u (include/Bingo.cuh:182-198): slot = current slot count,
@@ -219,7 +246,7 @@ struct ExactGraph {
       G.v.push_back(v);
     }
     ++X.live;
-    adj_add(X, v);
+    adj_add(X, v, w);
     return s;
   }
 
@@ -244,7 +271,7 @@ struct ExactGraph {
     }
     X.ew[s] = 0;
     --X.live;
-    adj_sub(X, X.ev[s]);
+    adj_sub(X, X.ev[s], w);
     return true;
   }
 
@@ -339,11 +366,20 @@ struct ExactGraph {
         if (!vx[cur].m) {
           x = -1;
         } else if (app == APP_NODE2VEC && prev >= 0) {
+          // Trial t: block (i, j, 2t+1) word y selects the return region,
+          // block (i, j, 2t) proposes, word x of (i, j, 2t+1) accepts.
+          const Vertex& C = vx[cur];
+          const uint64_t region =
+              region_threshold(th.ret_excess, adj_weight(C, (uint32_t)prev), C.alias[0].T);
           for (uint32_t t = 0;; ++t) {
+            const U4 a = philox4x32_10(U4{i, j, 2 * t + 1, job}, k0, k1);
+            if ((uint64_t)a.y < region) {
+              x = prev;
+              break;
+            }
             x = sample((uint32_t)cur, philox4x32_10(U4{i, j, 2 * t, job}, k0, k1));
             const uint64_t thr = x == prev ? th.ret : (adj_has(vx[prev], (uint32_t)x) ? th.in : th.out);
-            const uint32_t a = philox4x32_10(U4{i, j, 2 * t + 1, job}, k0, k1).x;
-            if ((uint64_t)a < thr || t + 1 == kMaxNode2vecTrials) break;
+            if ((uint64_t)a.x < thr || t + 1 == kMaxNode2vecTrials) break;
           }
         } else {
           x = sample((uint32_t)cur, philox4x32_10(U4{i, j, 0, job}, k0, k1));

@@ -24,9 +24,10 @@ int orc_alias_build(const uint64_t mass[32], uint64_t* thr, uint64_t* T, uint8_t
   return m;
 }
 
-void orc_walk_thresholds(double p, double q, double stop, uint64_t out[4]) {
+void orc_walk_thresholds(double p, double q, double stop, uint64_t out[4], double* excess) {
   oracle::WalkThresholds t = oracle::walk_thresholds(p, q, stop);
   out[0] = t.ret, out[1] = t.in, out[2] = t.out, out[3] = t.stop;
+  if (excess) *excess = t.ret_excess;
 }
 
 // ----- exact graph ---------------------------------------------------------

@@ -31,7 +31,7 @@ def lib():
         sig = {
             "orc_philox": (None, [vp, vp, vp]),
             "orc_alias_build": (c_int, [vp, vp, vp, vp, vp]),
-            "orc_walk_thresholds": (None, [c_double, c_double, c_double, vp]),
+            "orc_walk_thresholds": (None, [c_double, c_double, c_double, vp, vp]),
             "orc_new": (vp, [c_uint32]),
             "orc_free": (None, [vp]),
             "orc_load": (None, [vp, vp, vp, vp, c_uint64]),
@@ -88,8 +88,9 @@ def alias_build(mass32):
 
 def walk_thresholds(p, q, stop):
     o = np.zeros(4, np.uint64)
-    lib().orc_walk_thresholds(p, q, stop, _p(o))
-    return o
+    ex = np.zeros(1, np.float64)
+    lib().orc_walk_thresholds(p, q, stop, _p(o), _p(ex))
+    return o, float(ex[0])
 
 
 class ExactGraph:

@@ -76,3 +76,33 @@ def test_walk_transition_distribution_rmat():
     keys = set((src.astype(np.int64) << 32 | dst).tolist())
     pairs = (a[ok].astype(np.int64) << 32) | b[ok]
     assert all(x in keys for x in np.unique(pairs).tolist())
+
+
+@pytest.mark.parametrize("p,q", [(0.25, 4.0), (0.5, 2.0), (4.0, 0.25), (1.0, 1.0)])
+def test_node2vec_second_order_distribution(p, q):
+    """Second step of node2vec walks from a fixed (prev, cur) pair against
+    P(x) ~ w(cur, x) * alpha(prev, x), alpha = 1/p (x = prev), 1 (x a
+    neighbour of prev), 1/q (other). Covers the return region (1/p above the
+    envelope max(1, 1/q)) and plain rejection."""
+    from bingo_b200 import NODE2VEC
+    n = 16
+    # prev = 0 steps to cur = 1 almost surely; 0's other out-neighbours 2, 3
+    # make them "in" candidates at cur.
+    edges = [(0, 1, 2 ** 30), (0, 2, 1), (0, 3, 1),
+             (1, 0, 7), (1, 2, 3), (1, 3, 11), (1, 4, 5), (1, 5, 13)]
+    src = np.array([e[0] for e in edges], np.uint32)
+    dst = np.array([e[1] for e in edges], np.uint32)
+    w = np.array([e[2] for e in edges], np.uint32)
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    rows = g.walk(app=NODE2VEC, length=3, starts=np.zeros(1_000_000, np.uint32), p=p, q=q, seed=17)
+    rows = rows[rows[:, 1] == 1]
+    counts = np.bincount(rows[:, 2], minlength=n).astype(np.float64)
+    alpha = {0: 1 / p, 2: 1.0, 3: 1.0, 4: 1 / q, 5: 1 / q}
+    probs = np.zeros(n)
+    for (u, v, wt) in edges:
+        if u == 1:
+            probs[v] += wt * alpha[v]
+    probs /= probs.sum()
+    pv = _chisq(counts, probs)
+    assert pv > ALPHA, (p, q, pv, counts[:6] / counts.sum(), probs[:6])
