@@ -55,6 +55,27 @@ class BingoOp(ctypes.Structure):
     ]
 
 
+class BingoServeConfig(ctypes.Structure):
+    _fields_ = [
+        ("output_budget_bytes", c_uint64),
+        ("max_jobs", c_uint32),
+        ("max_update_batch", c_uint32),
+        ("idle_timeout_us", c_uint32),
+        ("reserved0", c_uint32),
+    ]
+
+
+class BingoServeStatus(ctypes.Structure):
+    _fields_ = [
+        ("done", c_int32),
+        ("status", c_int32),
+        ("kind", c_int32),
+        ("reserved0", c_int32),
+        ("version", c_uint64),
+        ("latency_ns", c_uint64),
+    ]
+
+
 class BingoStats(ctypes.Structure):
     _fields_ = [
         ("n", c_uint32),
@@ -83,6 +104,13 @@ SIGNATURES = {
     "bingo_walk_noalloc": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32]),
     "bingo_run": (c_int, [c_void_p, POINTER(BingoOp), c_uint32, c_uint32]),
     "bingo_sync": (c_int, [c_void_p]),
+    "bingo_serve_start": (c_int, [c_void_p, POINTER(BingoServeConfig)]),
+    "bingo_serve_submit_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), POINTER(c_uint64)]),
+    "bingo_serve_submit_update": (c_int, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p,
+                                          POINTER(c_uint64)]),
+    "bingo_serve_poll": (c_int, [c_void_p, c_uint64, POINTER(BingoServeStatus)]),
+    "bingo_serve_wait": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(BingoServeStatus)]),
+    "bingo_serve_stop": (c_int, [c_void_p]),
     "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
     "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),
     "bingo_dump_sizes": (c_int, [c_void_p, POINTER(c_uint64)]),
@@ -130,6 +158,7 @@ STATUS = {
     8: "BINGO_ERR_TIMEOUT",
     9: "BINGO_ERR_NO_DEVICE",
     10: "BINGO_ERR_UNSUPPORTED",
+    11: "BINGO_ERR_BUSY",
 }
 
 

@@ -6,6 +6,7 @@
 
 #include "../../include/bingo.h"
 #include "engine.cuh"
+#include "serve.cuh"
 
 struct bingo_handle {
   bingo::Engine* eng = nullptr;
@@ -16,9 +17,14 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// busy_ok: the call is allowed while the handle is serving.
 template <class F>
-int guarded(bingo_handle* h, F&& f) {
+int guarded(bingo_handle* h, F&& f, bool busy_ok = false) {
   if (!h || !h->eng) return BINGO_ERR_INVALID_ARGUMENT;
+  if (!busy_ok && h->eng->server()) {
+    h->eng->last_error = "the handle is serving (bingo_serve_stop first)";
+    return BINGO_ERR_BUSY;
+  }
   try {
     if (cudaSetDevice(h->device) != cudaSuccess) {
       cudaGetLastError();
@@ -82,6 +88,7 @@ int bingo_create(const bingo_config* cfg, bingo_handle** out) {
 }
 
 int bingo_destroy(bingo_handle* h) {
+  // A serving handle finishes its submitted requests first (engine destructor).
   if (!h) return BINGO_ERR_INVALID_ARGUMENT;
   cudaSetDevice(h->device);
   delete h->eng;
@@ -132,7 +139,62 @@ int bingo_set_stream(bingo_handle* h, void* stream) {
 
 int bingo_get_stats(bingo_handle* h, bingo_stats* out) {
   if (!out) return BINGO_ERR_INVALID_ARGUMENT;
-  return guarded(h, [&](bingo::Engine& e) { e.stats(out); });
+  return guarded(h, [&](bingo::Engine& e) { e.stats(out); }, true);
+}
+
+int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg) {
+  bingo_serve_config c{};
+  if (cfg) c = *cfg;
+  return guarded(h, [&](bingo::Engine& e) { e.serve_start(c); });
+}
+
+int bingo_serve_submit_walk(bingo_handle* h, const bingo_walk_job* job, uint64_t* ticket) {
+  if (!job || !ticket) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(
+      h,
+      [&](bingo::Engine& e) {
+        if (!e.server()) throw bingo::Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+        *ticket = e.server()->submit_walk(*job);
+      },
+      true);
+}
+
+int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, const uint32_t* b,
+                              const uint32_t* c, uint64_t k, uint32_t* out_slots, uint64_t* ticket) {
+  if (!ticket) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(
+      h,
+      [&](bingo::Engine& e) {
+        if (!e.server()) throw bingo::Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+        *ticket = e.server()->submit_update(kind, a, b, c, k, out_slots);
+      },
+      true);
+}
+
+int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out) {
+  return guarded(
+      h,
+      [&](bingo::Engine& e) {
+        if (!e.server()) throw bingo::Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+        e.server()->poll(ticket, out);
+      },
+      true);
+}
+
+int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out) {
+  int st = BINGO_OK;
+  const int g = guarded(
+      h,
+      [&](bingo::Engine& e) {
+        if (!e.server()) throw bingo::Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+        if (!e.server()->wait(ticket, timeout_us, out)) st = BINGO_ERR_TIMEOUT;
+      },
+      true);
+  return g ? g : st;
+}
+
+int bingo_serve_stop(bingo_handle* h) {
+  return guarded(h, [&](bingo::Engine& e) { e.serve_stop(); }, true);
 }
 
 int bingo_dump_sizes(bingo_handle* h, uint64_t sizes[3]) {

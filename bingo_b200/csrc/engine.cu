@@ -15,6 +15,7 @@
 #include <mutex>
 
 #include "engine.cuh"
+#include "serve.cuh"
 #include "store.cuh"
 #include "walk.cuh"
 
@@ -187,24 +188,6 @@ constexpr int walk_min_blocks(int app, bool multi) {
          : app == APP_PPR                           ? (multi ? 5 : 6)
          : app == APP_NODE2VEC                      ? (multi ? 4 : 5)
                                                     : 4;
-}
-
-__device__ __forceinline__ bool begin_any(const WalkView& W, const WalkJobDev& J, uint32_t i, LaneWalk& s,
-                                          RowStage& o, int32_t (*obuf)[8], uint32_t& mv) {
-  switch (J.app) {
-    case APP_DEEPWALK: return walk_begin<APP_DEEPWALK>(W, J, i, s, o, obuf, mv);
-    case APP_NODE2VEC: return walk_begin<APP_NODE2VEC>(W, J, i, s, o, obuf, mv);
-    case APP_PPR: return walk_begin<APP_PPR>(W, J, i, s, o, obuf, mv);
-    default: return walk_begin<APP_SAMPLING>(W, J, i, s, o, obuf, mv);
-  }
-}
-__device__ __forceinline__ bool advance_any(const WalkView& W, const WalkJobDev& J, LaneWalk& s, RowStage& o,
-                                            int32_t (*obuf)[8], uint32_t& mv) {
-  switch (J.app) {
-    case APP_DEEPWALK: return walk_advance<APP_DEEPWALK>(W, J, s, o, obuf, mv);
-    case APP_NODE2VEC: return walk_advance<APP_NODE2VEC>(W, J, s, o, obuf, mv);
-    default: return walk_advance<APP_PPR>(W, J, s, o, obuf, mv);
-  }
 }
 
 template <int APP, bool MULTI>
@@ -476,6 +459,7 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
 
 Engine::~Engine() {
   cudaSetDevice(cfg_.device);
+  server_.reset();
   if (stream_) cudaStreamSynchronize(stream_);
   drop_graph();
   prog_jobs_.release(), prog_prefix_.release(), prog_queue_.release();
@@ -854,14 +838,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   uint64_t s_total = 0, o_total = 0;
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const bingo_walk_job& J = jobs[j];
-    if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
-    if (J.app == BINGO_NODE2VEC && !cfg_.node2vec)
-      throw Error(BINGO_ERR_UNSUPPORTED, "node2vec needs the adjacency index (config.node2vec)");
-    if (J.app == BINGO_NODE2VEC && !(J.p > 0 && J.q > 0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "p, q must be > 0");
-    if (J.app == BINGO_PPR && !(J.stop_prob >= 0 && J.stop_prob <= 1))
-      throw Error(BINGO_ERR_INVALID_ARGUMENT, "stop_prob must be in [0, 1]");
-    if (J.app != BINGO_SAMPLING && J.length == 0 && J.n_starts)
-      throw Error(BINGO_ERR_INVALID_ARGUMENT, "length must be >= 1");
+    check_walk_job(J);
     if (J.n_starts && !J.out) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null output");
     if (J.n_starts >= (1ull << 32)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one job");
     if (J.starts) {
@@ -885,16 +862,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const bingo_walk_job& J = jobs[j];
     WalkJobDev& D = dj[j];
-    D.app = J.app;
-    D.L = J.length;
-    D.n = J.n_starts;
-    D.first = J.first;
-    D.job = J.job_id;
-    D.k0 = (uint32_t)J.seed;
-    D.k1 = (uint32_t)(J.seed >> 32);
-    D.flags = J.flags;
-    D.pad = 0;
-    set_thresholds(D, J);
+    D = make_job(J);
     D.starts = J.starts;
     if (s_off[j] != ~0ull) {
       uint32_t* d = wstart_.as<uint32_t>() + s_off[j];
@@ -976,6 +944,52 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
                                  cudaMemcpyDeviceToHost, stream_),
                  "walk D2H");
     }
+  finish_call();
+}
+
+// ------------------------------------------------------------------ jobs, serving
+void Engine::check_walk_job(const bingo_walk_job& J) const {
+  if (J.app < 0 || J.app > 3) throw Error(BINGO_ERR_INVALID_ARGUMENT, "unknown app");
+  if (J.app == BINGO_NODE2VEC && !cfg_.node2vec)
+    throw Error(BINGO_ERR_UNSUPPORTED, "node2vec needs the adjacency index (config.node2vec)");
+  if (J.app == BINGO_NODE2VEC && !(J.p > 0 && J.q > 0)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "p, q must be > 0");
+  if (J.app == BINGO_PPR && !(J.stop_prob >= 0 && J.stop_prob <= 1))
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "stop_prob must be in [0, 1]");
+  if (J.app != BINGO_SAMPLING && J.length == 0 && J.n_starts)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "length must be >= 1");
+}
+
+WalkJobDev Engine::make_job(const bingo_walk_job& J) const {
+  WalkJobDev D;
+  D.app = J.app;
+  D.L = J.length;
+  D.starts = J.starts;
+  D.n = J.n_starts;
+  D.first = J.first;
+  D.job = J.job_id;
+  D.k0 = (uint32_t)J.seed;
+  D.k1 = (uint32_t)(J.seed >> 32);
+  D.flags = J.flags;
+  D.pad = 0;
+  set_thresholds(D, J);
+  D.out = J.out;
+  return D;
+}
+
+void Engine::require_idle() const {
+  if (server_) throw Error(BINGO_ERR_BUSY, "the handle is serving (bingo_serve_stop first)");
+}
+
+void Engine::serve_start(const bingo_serve_config& cfg) {
+  require_loaded();
+  require_idle();
+  cuda_check(cudaStreamSynchronize(stream_), "serve start");
+  server_.reset(new Server(*this, cfg));
+}
+
+void Engine::serve_stop() {
+  if (!server_) throw Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+  server_.reset();
   finish_call();
 }
 
@@ -1326,6 +1340,11 @@ void Engine::philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, ui
 void Engine::stats(bingo_stats* out) {
   std::memset(out, 0, sizeof *out);
   out->n = n_;
+  if (server_) {  // the scheduler owns the stream and the host mirrors
+    cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
+    out->kernel_launches = launches_;
+    return;
+  }
   cuda_check(cudaStreamSynchronize(stream_), "stats");
   cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
   out->kernel_launches = launches_;

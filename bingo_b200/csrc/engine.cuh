@@ -3,6 +3,7 @@
 // apply) and launches the walk kernels.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -34,10 +35,14 @@ struct DevBuf {
   }
 };
 
+class Server;
+
 class Engine {
  public:
   explicit Engine(const bingo_config& cfg);
   ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
 
   void load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n);
   void insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
@@ -56,6 +61,20 @@ class Engine {
 
   std::string last_error;
   cudaStream_t stream() const { return stream_; }
+
+  // serving
+  void serve_start(const bingo_serve_config& cfg);
+  void serve_stop();
+  Server* server() const { return server_.get(); }
+  void require_idle() const;  // throws BINGO_ERR_BUSY while serving
+  // used by the serving scheduler
+  WalkView walk_view() const { return wview(); }
+  WalkJobDev make_job(const bingo_walk_job& J) const;
+  void check_walk_job(const bingo_walk_job& J) const;
+  void prepare_batches(uint64_t k) { ensure_batch_scratch(k); }
+  void count_launch() { ++launches_; }
+  uint32_t n() const { return n_; }
+  int device() const { return cfg_.device; }
 
  private:
   bingo_config cfg_;
@@ -87,6 +106,7 @@ class Engine {
   cudaGraphExec_t graph_exec_ = nullptr;
   uint64_t graph_sig_ = 0, graph_launches_ = 0;
   uint64_t arena_gen_ = 0;  // bumped whenever an arena or the vertex arrays are reallocated
+  std::unique_ptr<Server> server_;
 
   StoreView view() const;
   WalkView wview() const;

@@ -260,6 +260,24 @@ __device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev
   return !done;
 }
 
+__device__ __forceinline__ bool begin_any(const WalkView& W, const WalkJobDev& J, uint32_t i, LaneWalk& s,
+                                          RowStage& o, int32_t (*obuf)[8], uint32_t& mv) {
+  switch (J.app) {
+    case APP_DEEPWALK: return walk_begin<APP_DEEPWALK>(W, J, i, s, o, obuf, mv);
+    case APP_NODE2VEC: return walk_begin<APP_NODE2VEC>(W, J, i, s, o, obuf, mv);
+    case APP_PPR: return walk_begin<APP_PPR>(W, J, i, s, o, obuf, mv);
+    default: return walk_begin<APP_SAMPLING>(W, J, i, s, o, obuf, mv);
+  }
+}
+__device__ __forceinline__ bool advance_any(const WalkView& W, const WalkJobDev& J, LaneWalk& s, RowStage& o,
+                                            int32_t (*obuf)[8], uint32_t& mv) {
+  switch (J.app) {
+    case APP_DEEPWALK: return walk_advance<APP_DEEPWALK>(W, J, s, o, obuf, mv);
+    case APP_NODE2VEC: return walk_advance<APP_NODE2VEC>(W, J, s, o, obuf, mv);
+    default: return walk_advance<APP_PPR>(W, J, s, o, obuf, mv);
+  }
+}
+
 // One atomic per warp: adds the warp's produced steps to the running count.
 __device__ __forceinline__ void add_steps(const WalkView& W, unsigned long long mine) {
 #pragma unroll

@@ -14,7 +14,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import BingoConfig, BingoError, BingoOp, BingoStats, BingoWalkJob, lib
+from ._lib import (BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeStatus, BingoStats, BingoWalkJob,
+                   lib)
 
 DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
@@ -211,6 +212,68 @@ class Graph:
                                 job_id=job_id, seed=seed, flags=flags, p=p, q=q, stop_prob=stop_prob,
                                 out=out)], mode=mode)
         return out
+
+    # ------------------------------------------------------------ serving
+    def serve_start(self, output_budget_bytes: int = 1 << 30, max_jobs: int = 4096,
+                    max_update_batch: int = 1 << 20, idle_timeout_us: int = 2000):
+        """Start the continuous-batching walk server (bingo_serve_start)."""
+        cfg = BingoServeConfig(output_budget_bytes, max_jobs, max_update_batch, idle_timeout_us, 0)
+        self._check(self._L.bingo_serve_start(self._h, ctypes.byref(cfg)))
+        self._serve_keep = {}
+
+    def submit_walk(self, app: int = DEEPWALK, length: int = 80, starts=None, n_starts: Optional[int] = None,
+                    first: int = 0, seed: int = 0, job_id: int = 0, p: float = 0.5, q: float = 2.0,
+                    stop_prob: float = 0.0125, flags: int = 0, out=None):
+        """Submit one walk query; returns (ticket, out). out is filled when the ticket is done."""
+        if starts is not None:
+            n_starts = len(starts) if not hasattr(starts, "numel") else starts.numel()
+        if out is None:
+            out = np.empty((n_starts,) if app == SAMPLING else (n_starts, length), dtype=np.int32)
+        keep = []
+        job = self._job_array([WalkJob(app=app, length=length, starts=starts, n_starts=n_starts, first=first,
+                                       job_id=job_id, seed=seed, flags=flags, p=p, q=q, stop_prob=stop_prob,
+                                       out=out)], keep)
+        t = ctypes.c_uint64()
+        self._check(self._L.bingo_serve_submit_walk(self._h, job, ctypes.byref(t)))
+        self._serve_keep[t.value] = out
+        return t.value, out
+
+    def submit_update(self, kind: str, a, b, c=None, out_slots=None):
+        """Submit an insert (a = src, b = dst, c = weights) or delete (a = vertex,
+        b = slot) batch; returns (ticket, out_slots) (slots filled for inserts)."""
+        k = len(a) if not hasattr(a, "numel") else a.numel()
+        pa, ka = _u32(a)
+        pb, kb = _u32(b)
+        pc, kc = _u32(c) if c is not None else (None, None)
+        if kind == "insert" and out_slots is None:
+            out_slots = np.zeros(k, np.uint32)
+        po = _out(out_slots, np.uint32)[0] if out_slots is not None else None
+        t = ctypes.c_uint64()
+        self._check(self._L.bingo_serve_submit_update(self._h, OP_INSERT if kind == "insert" else OP_DELETE, pa, pb,
+                                                      pc, k, po, ctypes.byref(t)))
+        self._serve_keep[t.value] = out_slots
+        return t.value, out_slots
+
+    @staticmethod
+    def _status(s: BingoServeStatus) -> dict:
+        return {"done": bool(s.done), "status": s.status, "kind": s.kind, "version": s.version,
+                "latency_ns": s.latency_ns}
+
+    def serve_poll(self, ticket: int) -> dict:
+        s = BingoServeStatus()
+        self._check(self._L.bingo_serve_poll(self._h, ticket, ctypes.byref(s)))
+        return self._status(s)
+
+    def serve_wait(self, ticket: int, timeout_us: int = 20_000_000) -> dict:
+        """Wait for a ticket (bounded); raises BingoError(TIMEOUT) if it is not done in time."""
+        s = BingoServeStatus()
+        self._check(self._L.bingo_serve_wait(self._h, ticket, timeout_us, ctypes.byref(s)))
+        self._serve_keep.pop(ticket, None)
+        return self._status(s)
+
+    def serve_stop(self):
+        self._check(self._L.bingo_serve_stop(self._h))
+        self._serve_keep = {}
 
     def sync(self):
         self._check(self._L.bingo_sync(self._h))

@@ -39,7 +39,8 @@ typedef enum bingo_status {
   BINGO_ERR_NOT_LOADED = 7,       /* operation needs a loaded graph */
   BINGO_ERR_TIMEOUT = 8,          /* a bounded device wait expired */
   BINGO_ERR_NO_DEVICE = 9,        /* no usable CUDA device */
-  BINGO_ERR_UNSUPPORTED = 10      /* e.g. node2vec without the adjacency index */
+  BINGO_ERR_UNSUPPORTED = 10,     /* e.g. node2vec without the adjacency index */
+  BINGO_ERR_BUSY = 11             /* the handle is serving; only bingo_serve_* calls are allowed */
 } bingo_status;
 
 typedef enum bingo_app {
@@ -182,6 +183,49 @@ typedef struct bingo_op {
 #define BINGO_RUN_GRAPH 1u
 
 int bingo_run(bingo_handle* h, const bingo_op* ops, uint32_t n_ops, uint32_t flags);
+
+/* ---- Serving -----------------------------------------------------------
+ * Continuous batching of walk queries with interleaved update batches (the
+ * reference has no serving mode). Walk queries are admitted into a running
+ * device-resident walk loop as job slots and output memory free up, and
+ * their walks run mixed with those of every other admitted query. An update
+ * batch commits after every walk query submitted before it has finished,
+ * and before any query submitted after it starts, so a query sees the graph
+ * after exactly the updates submitted before it (its `version`), and its
+ * rows equal those of the same query run alone on that graph.
+ *
+ * Query inputs are copied at submit; `out` (host or device) must stay valid
+ * until the ticket is done. Admission: a query must fit the output budget
+ * (rows + starts), at most max_jobs queries are in flight. While serving,
+ * other calls on the handle return BINGO_ERR_BUSY. */
+typedef struct bingo_serve_config {
+  uint64_t output_budget_bytes; /* device memory for in-flight query rows and starts (default 1 GiB) */
+  uint32_t max_jobs;            /* queries in flight, <= 4096 (default 4096) */
+  uint32_t max_update_batch;    /* update batches apply in chunks of at most this many edges (default 2^20) */
+  uint32_t idle_timeout_us;     /* the walk loop exits after this long without work (default 2000) */
+  uint32_t reserved0;
+} bingo_serve_config;
+
+typedef struct bingo_serve_status {
+  int32_t done;        /* 1 when the request has finished */
+  int32_t status;      /* bingo_status of the request */
+  int32_t kind;        /* 0 walk, 1 insert, 2 delete */
+  int32_t reserved0;
+  uint64_t version;    /* updates applied before this request (walks) / including it (updates) */
+  uint64_t latency_ns; /* submit to result ready */
+} bingo_serve_status;
+
+int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg);
+int bingo_serve_submit_walk(bingo_handle* h, const bingo_walk_job* job, uint64_t* ticket);
+/* kind: BINGO_OP_INSERT (a = src, b = dst, c = weights, out_slots optional)
+ * or BINGO_OP_DELETE (a = vertex, b = slot). */
+int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, const uint32_t* b,
+                              const uint32_t* c, uint64_t k, uint32_t* out_slots, uint64_t* ticket);
+int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);
+/* Waits at most timeout_us; returns BINGO_ERR_TIMEOUT if the ticket is not done. */
+int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out);
+/* Finishes every submitted request, stops the walk loop, returns the handle to normal use. */
+int bingo_serve_stop(bingo_handle* h);
 
 /* Waits for all queued work; returns the first device-detected error since
  * the previous bingo_sync (or BINGO_OK). */

@@ -1,0 +1,109 @@
+"""Serving: walk queries admitted into a running device loop (continuous
+batching) with update batches interleaved. Every query's rows must equal the
+same query run alone on the graph version it saw (the updates submitted
+before it), checked against the CPU oracle replaying the stream in order."""
+import numpy as np
+import pytest
+
+from bingo_b200 import DEEPWALK, NODE2VEC, PPR, SAMPLING, BingoError, Graph, gen
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(scale=11, seed=81):
+    n = 1 << scale
+    src, dst = gen.rmat(scale, 16, seed=seed)
+    w = gen.weights(len(src), gen.W_UNIFORM, 1, 65535, seed=seed + 1)
+    return n, src, dst, w
+
+
+def test_served_results_equal_alone_results():
+    n, src, dst, w = _graph()
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    ex = po.ExactGraph(n)
+    ex.load(src, dst, w)
+    ug = gen.UpdateGen(n, src, dst, seed=85)
+    rng = np.random.default_rng(86)
+    g.serve_start(output_budget_bytes=64 << 20, idle_timeout_us=500)
+    trace = []
+    apps = [(DEEPWALK, 80, {}), (PPR, 80, dict(stop_prob=0.15)), (NODE2VEC, 40, dict(p=0.5, q=2.0)),
+            (SAMPLING, 1, {})]
+    for r in range(60):
+        if r % 7 == 6:
+            if r % 2:
+                ins = ug.inserts(int(rng.integers(1, 800)), gen.W_UNIFORM, 1, 65535)
+                t, slots = g.submit_update("insert", *ins)
+                trace.append(("insert", t, ins, slots))
+            else:
+                dels = ug.deletes(int(rng.integers(1, 800)))
+                t, _ = g.submit_update("delete", *dels)
+                trace.append(("delete", t, dels))
+        else:
+            app, L, kw = apps[r % len(apps)]
+            starts = rng.integers(0, n, size=int(rng.integers(1, 3000))).astype(np.uint32)
+            t, out = g.submit_walk(app=app, length=L, starts=starts, seed=1000 + r, job_id=r, **kw)
+            trace.append(("walk", t, (app, L, starts, r, kw), out))
+    results = {}
+    for item in trace:
+        results[item[1]] = g.serve_wait(item[1])
+    g.serve_stop()
+    version = 0
+    for item in trace:
+        st = results[item[1]]
+        assert st["done"] and st["status"] == 0, st
+        if item[0] == "walk":
+            app, L, starts, r, kw = item[2]
+            assert st["version"] == version
+            ref = ex.walk(app, L, starts, seed=1000 + r, job_id=r, p=kw.get("p", 0.5), q=kw.get("q", 2.0),
+                          stop=kw.get("stop_prob", 0.0125))
+            assert np.array_equal(item[3], ref), f"query {r} (app {app}) differs from its solo run"
+        elif item[0] == "insert":
+            version += 1
+            assert np.array_equal(item[3], ex.insert(*item[2]))
+        else:
+            version += 1
+            assert ex.delete(*item[2]) == 0
+    from tests.helpers import assert_exact_equal
+    assert_exact_equal(g.dump(), ex.dump())
+
+
+def test_continuous_batching_shares_launches():
+    """Many queries submitted back to back run inside a few walk-loop launches."""
+    n, src, dst, w = _graph(scale=12, seed=91)
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    g.serve_start(idle_timeout_us=20000)
+    l0 = g.stats()["kernel_launches"]
+    rng = np.random.default_rng(92)
+    tickets = [g.submit_walk(app=DEEPWALK, length=60, starts=rng.integers(0, n, size=500).astype(np.uint32),
+                             seed=i, job_id=i)[0] for i in range(200)]
+    for t in tickets:
+        assert g.serve_wait(t)["status"] == 0
+    launches = g.stats()["kernel_launches"] - l0
+    g.serve_stop()
+    assert launches <= 20, launches
+
+
+def test_admission_by_budget_and_busy_guard():
+    n, src, dst, w = _graph(scale=10, seed=95)
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    g.serve_start(output_budget_bytes=1 << 20)  # 1 MiB: a 5000 x 80 query needs 1.6 MB
+    with pytest.raises(BingoError) as e:
+        g.submit_walk(app=DEEPWALK, length=80, starts=np.zeros(5000, np.uint32))
+    assert e.value.name == "BINGO_ERR_CAPACITY"
+    # queries that fit one at a time are admitted as memory frees up
+    tickets = [g.submit_walk(app=DEEPWALK, length=80, starts=np.full(2000, i, np.uint32), seed=i, job_id=i)
+               for i in range(12)]
+    with pytest.raises(BingoError) as e:
+        g.walk(app=DEEPWALK, length=8, starts=[0])
+    assert e.value.name == "BINGO_ERR_BUSY"
+    ex = po.ExactGraph(n)
+    ex.load(src, dst, w)
+    for i, (t, out) in enumerate(tickets):
+        assert g.serve_wait(t)["status"] == 0
+        assert np.array_equal(out, ex.walk(DEEPWALK, 80, np.full(2000, i, np.uint32), seed=i, job_id=i))
+    g.serve_stop()
+    g.walk(app=DEEPWALK, length=8, starts=[0])  # usable again
