@@ -341,6 +341,150 @@ def run_batched(args):
         print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- served (config 5)
+S_SEED = 1234 + 5
+
+
+def make_trace(rng, n, walkable, ug, n_req, rate, p_update):
+    """Poisson arrivals at `rate` requests/s. A request is an update batch
+    (probability p_update; log-uniform 1..1M edges; insert or delete with
+    equal odds) or a walk query (log-uniform 1..100K starts over vertices with
+    out-edges, length 80, DeepWalk or PPR with stop 0.15)."""
+    from bingo_b200 import DEEPWALK, PPR, gen
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    reqs = []
+    for i in range(n_req):
+        if rng.random() < p_update:
+            k = int(np.exp(rng.uniform(0, np.log(1e6))))
+            if rng.random() < 0.5:
+                reqs.append(("insert", t[i], ug.inserts(k, gen.W_LOGUNIFORM, 1, 2 ** 32 - 1)))
+            else:
+                reqs.append(("delete", t[i], ug.deletes(k)))
+        else:
+            k = int(np.exp(rng.uniform(0, np.log(1e5))))
+            app = DEEPWALK if rng.random() < 0.5 else PPR
+            reqs.append(("walk", t[i], (app, rng.choice(walkable, size=k).astype(np.uint32), i)))
+    return reqs
+
+
+def pct(xs, q):
+    return float(np.percentile(np.asarray(xs, np.float64), q)) if len(xs) else None
+
+
+def run_served(args):
+    import torch
+    from bingo_b200 import Graph, gen
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    scale = args.served_scale
+    n = 1 << scale
+    src, dst = gen.rmat(scale, EDGE_FACTOR, seed=S_SEED)
+    w = gen.weights(len(src), gen.W_LOGUNIFORM, 1, 2 ** 32 - 1, seed=S_SEED + 1)
+    walkable = np.nonzero(np.bincount(src, minlength=n))[0].astype(np.uint32)
+    ug = gen.UpdateGen(n, src, dst, seed=S_SEED + 2)
+    rng = np.random.default_rng(S_SEED + 3)
+    rates = [float(x) for x in args.rates.split(",")]
+    traces = [make_trace(rng, n, walkable, ug, args.requests, r, args.p_update) for r in rates]
+    g = Graph(device=local, node2vec=False, arena_factor=1.25)
+
+    def prepare(upto):
+        """Base graph plus the update batches of every earlier trace."""
+        g.load_edges(src, dst, w, n)
+        for tr in traces[:upto]:
+            for kind, _, x in tr:
+                if kind == "insert":
+                    g.insert_batch(*x, return_slots=False)
+                elif kind == "delete":
+                    g.delete_batch(*x)
+
+    def outputs(tr):
+        tot = sum(len(x[1]) * WALK_LEN for kind, _, x in tr if kind == "walk")
+        pool = torch.empty(max(tot, 1), dtype=torch.int32).pin_memory()
+        outs, off = [], 0
+        for kind, _, x in tr:
+            if kind == "walk":
+                k = len(x[1])
+                outs.append(pool[off:off + k * WALK_LEN].view(k, WALK_LEN))
+                off += k * WALK_LEN
+            else:
+                outs.append(None)
+        return outs
+
+    results = []
+    for ri, (rate, tr) in enumerate(zip(rates, traces)):
+        outs = outputs(tr)
+        # ---- served: continuous batching
+        prepare(ri)
+        s0 = g.stats()["walk_steps"]
+        g.serve_start(output_budget_bytes=args.serve_budget << 20, max_update_batch=1 << 20, idle_timeout_us=3000)
+        t0 = time.monotonic_ns()
+        tickets = []
+        for (kind, at, x), out in zip(tr, outs):
+            due = t0 + int(at * 1e9)
+            while time.monotonic_ns() < due:
+                pass
+            if kind == "walk":
+                app, starts, jid = x
+                tickets.append((kind, due, g.submit_walk(app=app, length=WALK_LEN, starts=starts, seed=7,
+                                                         job_id=jid, stop_prob=0.15, out=out)[0]))
+            else:
+                tickets.append((kind, due, g.submit_update(kind, *x)[0]))
+        lat = {"walk": [], "update": []}
+        last_ready = t0
+        for kind, due, t in tickets:
+            st = g.serve_wait(t, timeout_us=600_000_000)
+            assert st["status"] == 0, st
+            lat["walk" if kind == "walk" else "update"].append((st["ready_ns"] - due) / 1e6)
+            last_ready = max(last_ready, st["ready_ns"])
+        smet = g.serve_metrics()
+        g.serve_stop()
+        served_steps = g.stats()["walk_steps"] - s0
+        served_span = (last_ready - t0) / 1e9
+        # ---- plain: one request at a time in arrival order (a queue, no batching)
+        prepare(ri)
+        s0 = g.stats()["walk_steps"]
+        plat = {"walk": [], "update": []}
+        t0 = time.monotonic_ns()
+        for (kind, at, x), out in zip(tr, outs):
+            due = t0 + int(at * 1e9)
+            while time.monotonic_ns() < due:
+                pass
+            if kind == "walk":
+                app, starts, jid = x
+                g.walk(app=app, length=WALK_LEN, starts=starts, seed=7, job_id=jid, stop_prob=0.15, out=out)
+            elif kind == "insert":
+                g.insert_batch(*x, return_slots=False)
+            else:
+                g.delete_batch(*x)
+            plat["walk" if kind == "walk" else "update"].append((time.monotonic_ns() - due) / 1e6)
+        plain_span = (time.monotonic_ns() - t0) / 1e9
+        plain_steps = g.stats()["walk_steps"] - s0
+        n_walk = len(lat["walk"])
+        upd_edges = sum(len(x[0]) for kind, _, x in tr if kind != "walk")
+        results.append({
+            "rate_req_s": rate, "requests": len(tr), "walk_queries": n_walk, "update_batches": len(tr) - n_walk,
+            "update_edges": upd_edges,
+            "served": {"walk_p50_ms": pct(lat["walk"], 50), "walk_p99_ms": pct(lat["walk"], 99),
+                       "update_p50_ms": pct(lat["update"], 50), "update_p99_ms": pct(lat["update"], 99),
+                       "walk_steps_per_s": served_steps / served_span, "requests_per_s": len(tr) / served_span,
+                       "span_s": served_span, "scheduler": smet},
+            "plain": {"walk_p50_ms": pct(plat["walk"], 50), "walk_p99_ms": pct(plat["walk"], 99),
+                      "update_p50_ms": pct(plat["update"], 50), "update_p99_ms": pct(plat["update"], 99),
+                      "walk_steps_per_s": plain_steps / plain_span, "requests_per_s": len(tr) / plain_span,
+                      "span_s": plain_span},
+        })
+    best = max(results, key=lambda r: r["served"]["walk_steps_per_s"])
+    line = {"metric": "walk_steps_per_s", "value": best["served"]["walk_steps_per_s"], "unit": "steps/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"served-rmat{scale}", "scale": scale, "m": int(len(src)),
+                       "weights": "loguniform[1,2^32)", "p_update": args.p_update, "walk_len": WALK_LEN,
+                       "requests_per_rate": args.requests, "serve_budget_mb": args.serve_budget,
+                       "latency": "arrival (scheduled) to result in pinned host memory"},
+            "sweep": results}
+    print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- reference CUDA build
 REF_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
@@ -631,8 +775,14 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
-                    help="plain: BASELINE config 2 (default); batched: config 4, batched vs plain")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: BASELINE config 2 (default); batched: config 4, batched vs plain; "
+                         "served: config 5, Poisson request stream, served vs plain")
+    ap.add_argument("--served-scale", type=int, default=24)
+    ap.add_argument("--rates", default="500,2000,8000", help="served: request rates (req/s) to sweep")
+    ap.add_argument("--requests", type=int, default=400, help="served: requests per rate")
+    ap.add_argument("--p-update", type=float, default=0.05, help="served: fraction of update requests")
+    ap.add_argument("--serve-budget", type=int, default=4096, help="served: output budget in MiB")
     ap.add_argument("--cpu-walks", type=int, default=131072)
     ap.add_argument("--ref-walks", type=int, default=131072)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
@@ -644,6 +794,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.workload == "batched" and args.impl == "ours":
         run_batched(args)
+    elif args.workload == "served" and args.impl == "ours":
+        run_served(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-cuda":

@@ -73,7 +73,14 @@ class BingoServeStatus(ctypes.Structure):
         ("reserved0", c_int32),
         ("version", c_uint64),
         ("latency_ns", c_uint64),
+        ("ready_ns", c_uint64),
     ]
+
+
+class BingoServeMetrics(ctypes.Structure):
+    _fields_ = [(f, c_uint64) for f in ("submitted", "completed", "walk_kernel_launches", "scheduler_passes",
+                                         "admit_ns", "complete_ns", "update_ns", "drain_wait_ns", "max_inflight",
+                                         "queue_ns", "device_ns", "copy_ns", "drain_inflight_ns")]
 
 
 class BingoStats(ctypes.Structure):
@@ -111,6 +118,7 @@ SIGNATURES = {
     "bingo_serve_poll": (c_int, [c_void_p, c_uint64, POINTER(BingoServeStatus)]),
     "bingo_serve_wait": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(BingoServeStatus)]),
     "bingo_serve_stop": (c_int, [c_void_p]),
+    "bingo_serve_get_metrics": (c_int, [c_void_p, POINTER(BingoServeMetrics)]),
     "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
     "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),
     "bingo_dump_sizes": (c_int, [c_void_p, POINTER(c_uint64)]),

@@ -193,6 +193,17 @@ int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bing
   return g ? g : st;
 }
 
+int bingo_serve_get_metrics(bingo_handle* h, bingo_serve_metrics* out) {
+  if (!out) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(
+      h,
+      [&](bingo::Engine& e) {
+        if (!e.server()) throw bingo::Error(BINGO_ERR_INVALID_ARGUMENT, "not serving");
+        e.server()->metrics(out);
+      },
+      true);
+}
+
 int bingo_serve_stop(bingo_handle* h) {
   return guarded(h, [&](bingo::Engine& e) { e.serve_stop(); }, true);
 }

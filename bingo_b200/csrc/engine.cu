@@ -970,7 +970,7 @@ WalkJobDev Engine::make_job(const bingo_walk_job& J) const {
   D.k0 = (uint32_t)J.seed;
   D.k1 = (uint32_t)(J.seed >> 32);
   D.flags = J.flags;
-  D.pad = 0;
+  D.seq = 0;
   set_thresholds(D, J);
   D.out = J.out;
   return D;
@@ -1147,7 +1147,7 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
       D.k0 = (uint32_t)J.seed;
       D.k1 = (uint32_t)(J.seed >> 32);
       D.flags = J.flags;
-      D.pad = 0;
+      D.seq = 0;
       set_thresholds(D, J);
       D.out = J.out;
       dj.push_back(D);
@@ -1299,7 +1299,7 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
     D.k0 = (uint32_t)J.seed;
     D.k1 = (uint32_t)(J.seed >> 32);
     D.flags = J.flags;
-    D.pad = 0;
+    D.seq = 0;
     set_thresholds(D, J);
     D.out = J.out;
   }

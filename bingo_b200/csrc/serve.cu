@@ -7,11 +7,15 @@
 // (FIFO versioning), so its result equals the result of running it alone on
 // that graph version (walks are keyed by (walk, step, trial, job) only).
 //
-// Device side: k_serve polls a control block in mapped pinned host memory
-// with a bounded, backed-off spin and exits after an idle limit (the host
-// relaunches it when work arrives). Items are claimed with a CAS bounded by
-// the published item count; each lane copies its job's descriptor into
-// shared memory through L2 (ring slots are reused while the kernel runs, and
+// Device side: k_serve polls a control block in device memory (the host
+// publishes with stream-ordered copies: a job's descriptor lands before the
+// count that exposes it) with a bounded, exponentially backed-off spin and
+// closes as a whole after an idle time limit (the host relaunches it when
+// work arrives).
+// Walks are claimed 32 at a time by fetch-add on a per-job counter tagged
+// with the job's sequence number (no compare-and-swap loop across thousands
+// of warps); each lane copies its job's descriptor into shared memory
+// through L2 (ring slots are reused while the kernel runs, and
 // L1 is not coherent); the lane that finishes a job's last walk fences and
 // writes the job's sequence number + 1 to a completion word in mapped memory.
 //
@@ -33,18 +37,57 @@ namespace bingo {
 namespace {
 
 constexpr int kServeBlock = 256;
+constexpr uint32_t kPollSteps = 8;
+
+// Lane 0 of a warp: take up to 32 walks of the oldest job that has any left.
+// Returns the count taken (0: none now); *none_left is set when every
+// published job is fully handed out.
+__device__ __forceinline__ uint32_t claim_walks(const WalkJobDev* __restrict__ jobs, const ServeCtl* ctl,
+                                                ServeDevState* st, volatile unsigned long long* err_word,
+                                                uint32_t* job, uint32_t* first, bool* none_left) {
+  volatile ServeDevState* vs = st;
+  *none_left = false;
+  for (int tries = 0; tries < 4; ++tries) {
+    const uint32_t h = vs->head_job;
+    const uint32_t pj = ctl->published_jobs;
+    if ((int32_t)(pj - h) <= 0) {
+      *none_left = true;
+      return 0;
+    }
+    const uint32_t slot = h & (kServeMaxJobs - 1);
+    const unsigned long long old = atomicAdd(&st->claim[slot], 32ull);
+    if ((uint32_t)(old >> 32) != h) return 0;  // its predecessor's advancer has not opened it yet
+    const uint32_t c = (uint32_t)old;
+    const unsigned long long n = __ldcg(&jobs[slot].n);
+    if (__ldcg(&jobs[slot].seq) != h) {  // the slot was reused under a claim: never expected
+      *err_word = 1;
+      __threadfence_system();
+      return 0;
+    }
+    if (c < n) {
+      *job = h;
+      *first = c;
+      return (uint32_t)min(32ull, n - c);
+    }
+    // Exhausted: move head_job past it and open the next job's counter.
+    if (atomicCAS(&st->head_job, h, h + 1) == h)
+      atomicExch(&st->claim[(h + 1) & (kServeMaxJobs - 1)], (unsigned long long)(h + 1) << 32);
+  }
+  return 0;
+}
 
 __global__ void __launch_bounds__(kServeBlock, 4)
-    k_serve(WalkView W, const WalkJobDev* __restrict__ jobs, const unsigned long long* __restrict__ base,
-            ServeCtl* ctl, ServeDevState* st, volatile unsigned long long* done_seq, uint32_t idle_limit) {
+    k_serve(WalkView W, const WalkJobDev* __restrict__ jobs, const ServeCtl* ctl, ServeDevState* st,
+            volatile unsigned long long* done_seq, volatile unsigned long long* err_word, uint32_t idle_us) {
   __shared__ __align__(16) int32_t obuf[kServeBlock][8];
   __shared__ __align__(16) WalkJobDev jc[kServeBlock];
   const int lane = threadIdx.x & 31;
   WalkJobDev& J = jc[threadIdx.x];
   LaneWalk s;
   RowStage o{kNoSec, 0};
-  uint32_t moves = 0, jseq = 0, idle_iters = 0;
-  unsigned long long wb = 0, we = 0;
+  uint32_t moves = 0, jseq = 0, nap = 256, poll_in = 0;
+  unsigned long long idle_ns = 0;
+  uint32_t wj = 0, wb = 0, we = 0;  // this warp's claimed range: walks [wb, we) of job wj
   bool active = false;
 
   auto finish = [&]() {
@@ -58,65 +101,66 @@ __global__ void __launch_bounds__(kServeBlock, 4)
 
   for (;;) {
     uint32_t idle = __ballot_sync(kFull, !active);
+    // A warp that still has walks in flight asks for more only when half its
+    // lanes are idle or every kPollSteps steps.
+    const bool may_claim = idle == kFull || __popc(idle) >= 16 || poll_in == 0;
+    poll_in = poll_in ? poll_in - 1 : kPollSteps;
+    int none_left = 0;
     while (idle) {
       if (wb >= we) {
-        unsigned long long cur = 0, got = 0;
+        if (!may_claim) break;
+        uint32_t cj = 0, cb = 0, got = 0;
         if (lane == 0) {
-          cur = *reinterpret_cast<volatile unsigned long long*>(&st->next_item);
-          const unsigned long long pub = ctl->published_items;
-          while (cur < pub) {
-            const unsigned long long take = min((unsigned long long)32, pub - cur);
-            const unsigned long long old = atomicCAS(&st->next_item, cur, cur + take);
-            if (old == cur) {
-              got = take;
-              break;
-            }
-            cur = old;
-          }
+          bool nl = false;
+          got = claim_walks(jobs, ctl, st, err_word, &cj, &cb, &nl);
+          none_left = nl;
         }
-        cur = __shfl_sync(kFull, cur, 0);
         got = __shfl_sync(kFull, got, 0);
-        if (!got) break;
-        wb = cur;
-        we = cur + got;
+        if (!got) {
+          none_left = __shfl_sync(kFull, none_left, 0);
+          break;
+        }
+        wj = __shfl_sync(kFull, cj, 0);
+        wb = __shfl_sync(kFull, cb, 0);
+        we = wb + got;
       }
-      const uint32_t take = (uint32_t)min((unsigned long long)__popc(idle), we - wb);
+      const uint32_t take = min((uint32_t)__popc(idle), we - wb);
       const uint32_t rank = __popc(idle & lanemask_lt());
       if (!active && rank < take) {
-        const unsigned long long item = wb + rank;
-        uint32_t lo = ctl->oldest_job, hi = ctl->published_jobs;
-        while (hi - lo > 1) {
-          const uint32_t mid = lo + ((hi - lo) >> 1);
-          if (__ldcg(base + (mid & (kServeMaxJobs - 1))) <= item)
-            lo = mid;
-          else
-            hi = mid;
-        }
-        jseq = lo;
-        const uint32_t slot = lo & (kServeMaxJobs - 1);
-        const int4* src = reinterpret_cast<const int4*>(jobs + slot);
+        jseq = wj;
+        const int4* src = reinterpret_cast<const int4*>(jobs + (wj & (kServeMaxJobs - 1)));
         int4* dst = reinterpret_cast<int4*>(&J);
 #pragma unroll
         for (int t = 0; t < (int)(sizeof(WalkJobDev) / 16); ++t) dst[t] = __ldcg(src + t);
-        const uint32_t i = (uint32_t)(item - __ldcg(base + slot));
-        active = begin_any(W, J, i, s, o, obuf, moves);
+        active = begin_any(W, J, wb + rank, s, o, obuf, moves);
         if (!active) finish();
       }
       wb += take;
       idle = __ballot_sync(kFull, !active);
     }
     if (!__any_sync(kFull, active)) {
+      // Idle warp (its last claim attempt just ran): exit on drain, stop or a
+      // closing kernel; after the idle limit, close the whole kernel (only
+      // while nothing is unclaimed), so the host never sees a kernel that
+      // runs on with a few warps left.
       int quit = 0;
       if (lane == 0) {
-        const unsigned long long nx = *reinterpret_cast<volatile unsigned long long*>(&st->next_item);
-        quit = (ctl->drain && nx >= ctl->published_items) || ctl->stop;
+        volatile ServeDevState* vs = st;
+        quit = (ctl->drain && none_left) || ctl->stop || vs->closing;
+        if (!quit && none_left && idle_ns > (unsigned long long)idle_us * 1000) {
+          atomicExch(&st->closing, 1u);
+          quit = 1;
+        }
       }
       quit = __shfl_sync(kFull, quit, 0);
-      if (quit || ++idle_iters > idle_limit) break;
-      __nanosleep(1000);
+      if (quit) break;
+      __nanosleep(nap);
+      idle_ns += nap;
+      nap = min(nap * 2, 16384u);
       continue;
     }
-    idle_iters = 0;
+    nap = 256;
+    idle_ns = 0;
     if (active) {
       active = advance_any(W, J, s, o, obuf, moves);
       if (!active) finish();
@@ -151,6 +195,7 @@ struct Server::InFlight {
   size_t out_bytes;
   bool copying = false;
   cudaEvent_t ev = nullptr;
+  uint64_t admit_ns = 0, device_done_ns = 0;
 };
 
 Server::Server(Engine& eng, const bingo_serve_config& cfg) : eng_(eng), cfg_(cfg) {
@@ -159,16 +204,18 @@ Server::Server(Engine& eng, const bingo_serve_config& cfg) : eng_(eng), cfg_(cfg
   if (!cfg_.max_update_batch) cfg_.max_update_batch = 1u << 20;
   if (!cfg_.idle_timeout_us) cfg_.idle_timeout_us = 2000;
   cuda_check(cudaStreamCreateWithFlags(&kstream_, cudaStreamNonBlocking), "serve stream");
-  cuda_check(cudaStreamCreateWithFlags(&cstream_, cudaStreamNonBlocking), "serve copy stream");
-  cuda_check(cudaHostAlloc((void**)&ctl_, sizeof(ServeCtl), cudaHostAllocMapped), "serve control block");
-  cuda_check(cudaHostAlloc((void**)&done_seq_, kServeMaxJobs * sizeof(unsigned long long), cudaHostAllocMapped),
+  cuda_check(cudaStreamCreateWithFlags(&cstream_, cudaStreamNonBlocking), "serve publish stream");
+  cuda_check(cudaStreamCreateWithFlags(&rstream_, cudaStreamNonBlocking), "serve result stream");
+  cuda_check(cudaHostAlloc((void**)&pin_, kPinBytes, cudaHostAllocDefault), "serve staging");
+  cuda_check(cudaHostAlloc((void**)&done_seq_, (kServeMaxJobs + 1) * sizeof(unsigned long long), cudaHostAllocMapped),
              "serve completion words");
-  std::memset((void*)ctl_, 0, sizeof(ServeCtl));
-  std::memset((void*)done_seq_, 0, kServeMaxJobs * sizeof(unsigned long long));
-  cuda_check(cudaHostGetDevicePointer((void**)&d_ctl_, (void*)ctl_, 0), "serve control block");
+  std::memset((void*)done_seq_, 0, (kServeMaxJobs + 1) * sizeof(unsigned long long));
   cuda_check(cudaHostGetDevicePointer((void**)&d_done_seq_, (void*)done_seq_, 0), "serve completion words");
+  ctlbuf_.ensure(sizeof(ServeCtl), "serve control block");
+  d_ctl_ = ctlbuf_.as<ServeCtl>();
+  std::memset(&ctl_, 0, sizeof ctl_);
+  cuda_check(cudaMemcpy(d_ctl_, &ctl_, sizeof ctl_, cudaMemcpyHostToDevice), "serve control block");
   jobs_.ensure(kServeMaxJobs * sizeof(WalkJobDev), "serve job ring");
-  base_.ensure(kServeMaxJobs * sizeof(unsigned long long), "serve job ring");
   state_.ensure(sizeof(ServeDevState), "serve state");
   cuda_check(cudaMemset(state_.p, 0, sizeof(ServeDevState)), "serve state");
   budget_.ensure(cfg_.output_budget_bytes, "serve output budget");
@@ -185,13 +232,16 @@ Server::~Server() {
   if (thread_.joinable()) thread_.join();
   cudaStreamSynchronize(kstream_);
   cudaStreamSynchronize(cstream_);
+  cudaStreamSynchronize(rstream_);
   for (auto& f : inflight_)
     if (f.ev) cudaEventDestroy(f.ev);
-  jobs_.release(), base_.release(), state_.release(), budget_.release();
-  cudaFreeHost((void*)ctl_);
+  for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
+  cudaFreeHost(pin_);
+  jobs_.release(), state_.release(), budget_.release(), ctlbuf_.release();
   cudaFreeHost((void*)done_seq_);
   cudaStreamDestroy(kstream_);
   cudaStreamDestroy(cstream_);
+  cudaStreamDestroy(rstream_);
 }
 
 uint64_t Server::submit_walk(const bingo_walk_job& J) {
@@ -210,7 +260,10 @@ uint64_t Server::submit_walk(const bingo_walk_job& J) {
   r.job = J;
   if (J.starts) {
     r.a.resize(J.n_starts);
-    cuda_check(cudaMemcpy(r.a.data(), J.starts, J.n_starts * 4, cudaMemcpyDefault), "copy starts");
+    if (is_device_ptr(J.starts))
+      cuda_check(cudaMemcpy(r.a.data(), J.starts, J.n_starts * 4, cudaMemcpyDeviceToHost), "copy starts");
+    else
+      std::memcpy(r.a.data(), J.starts, J.n_starts * 4);
     for (uint32_t v : r.a)
       if (v >= eng_.n()) throw Error(BINGO_ERR_OUT_OF_RANGE, "start id >= n");
   } else if ((uint64_t)J.first + J.n_starts > eng_.n()) {
@@ -225,14 +278,17 @@ uint64_t Server::submit_update(int kind, const uint32_t* a, const uint32_t* b, c
   if (k && (!a || !b || (kind == BINGO_OP_INSERT && !c))) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null batch array");
   Request r;
   r.kind = kind;
-  r.a.resize(k), r.b.resize(k);
+  auto grab = [&](std::vector<uint32_t>& dst, const uint32_t* src) {
+    dst.resize(k);
+    if (is_device_ptr(src))
+      cuda_check(cudaMemcpy(dst.data(), src, k * 4, cudaMemcpyDeviceToHost), "copy batch");
+    else
+      std::memcpy(dst.data(), src, k * 4);
+  };
   if (k) {
-    cuda_check(cudaMemcpy(r.a.data(), a, k * 4, cudaMemcpyDefault), "copy batch");
-    cuda_check(cudaMemcpy(r.b.data(), b, k * 4, cudaMemcpyDefault), "copy batch");
-    if (kind == BINGO_OP_INSERT) {
-      r.c.resize(k);
-      cuda_check(cudaMemcpy(r.c.data(), c, k * 4, cudaMemcpyDefault), "copy batch");
-    }
+    grab(r.a, a);
+    grab(r.b, b);
+    if (kind == BINGO_OP_INSERT) grab(r.c, c);
   }
   r.out_slots = out_slots;
   return enqueue(std::move(r));
@@ -261,6 +317,7 @@ bool Server::poll(uint64_t ticket, bingo_serve_status* out) {
     out->status = t.status;
     out->version = t.version;
     out->latency_ns = t.done ? t.done_ns - t.submit_ns : 0;
+    out->ready_ns = t.done ? t.done_ns : 0;
     out->kind = t.kind;
   }
   return t.done;
@@ -342,31 +399,50 @@ void Server::launch_kernel() {
     cudaGetLastError();
     per_sm = 2;
   }
-  const uint32_t idle_limit = cfg_.idle_timeout_us;  // ~1 us per idle iteration
-  k_serve<<<sms * per_sm, kServeBlock, 0, kstream_>>>(eng_.walk_view(), jobs_.as<WalkJobDev>(),
-                                                       base_.as<unsigned long long>(), d_ctl_,
-                                                       state_.as<ServeDevState>(), d_done_seq_, idle_limit);
+  cuda_check(cudaMemsetAsync(&state_.as<ServeDevState>()->closing, 0, 4, kstream_), "serve launch");
+  k_serve<<<sms * per_sm, kServeBlock, 0, kstream_>>>(eng_.walk_view(), jobs_.as<WalkJobDev>(), d_ctl_,
+                                                       state_.as<ServeDevState>(), d_done_seq_,
+                                                       d_done_seq_ + kServeMaxJobs, cfg_.idle_timeout_us);
   cuda_check(cudaGetLastError(), "serving kernel launch");
   eng_.count_launch();
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    ++m_.walk_kernel_launches;
+  }
   launched_ = true;
 }
 
 // One pass of the scheduler; returns true if anything progressed.
 bool Server::step() {
   bool progress = false;
+  const uint64_t t_begin = now_ns();
   // ---- completions (in any order), copies, retirement (in order)
   for (auto& f : inflight_) {
     if (!f.copying && done_seq_[f.seq & (kServeMaxJobs - 1)] == (unsigned long long)f.seq + 1) {
-      cuda_check(cudaMemcpyAsync(f.host_out, f.dev_out, f.out_bytes, cudaMemcpyDefault, cstream_), "result copy");
-      cuda_check(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming), "event");
-      cuda_check(cudaEventRecord(f.ev, cstream_), "event");
+      cuda_check(cudaMemcpyAsync(f.host_out, f.dev_out, f.out_bytes, cudaMemcpyDefault, rstream_), "result copy");
+      if (event_pool_.empty()) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        event_pool_.push_back(e);
+      }
+      f.ev = event_pool_.back();
+      event_pool_.pop_back();
+      cuda_check(cudaEventRecord(f.ev, rstream_), "event");
       f.copying = true;
+      f.device_done_ns = now_ns();
       progress = true;
     }
   }
   for (auto it = inflight_.begin(); it != inflight_.end();) {
     if (it->copying && cudaEventQuery(it->ev) == cudaSuccess) {
-      cudaEventDestroy(it->ev);
+      event_pool_.push_back(it->ev);
+      it->ev = nullptr;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        const uint64_t t = now_ns();
+        m_.device_ns += it->device_done_ns - it->admit_ns;
+        m_.copy_ns += t - it->device_done_ns;
+      }
       finish_ticket(it->ticket, BINGO_OK, version_);
       release_region(it->off);
       retired_.insert(it->seq);
@@ -376,10 +452,11 @@ bool Server::step() {
       ++it;
     }
   }
+  const uint64_t t_completed = now_ns();
+  if (done_seq_[kServeMaxJobs]) throw Error(BINGO_ERR_CUDA, "serving kernel met a reused job slot");
   while (retired_.count(oldest_)) {
     retired_.erase(oldest_);
     ++oldest_;
-    ctl_->oldest_job = oldest_;
   }
   // ---- admission in submission order
   for (;;) {
@@ -390,6 +467,7 @@ bool Server::step() {
       r = &queue_.front();
     }
     if (r->kind == 0) {
+      const uint64_t t_adm = now_ns();
       const bingo_walk_job& J = r->job;
       if (published_jobs_ - oldest_ >= cfg_.max_jobs) break;
       const uint64_t per = J.app == BINGO_SAMPLING ? 1 : J.length;
@@ -401,42 +479,60 @@ bool Server::step() {
       uint32_t* dev_starts = sb ? reinterpret_cast<uint32_t*>(budget_.as<char>() + off + ob) : nullptr;
       const uint32_t seq = published_jobs_;
       const uint32_t slot = seq & (kServeMaxJobs - 1);
-      WalkJobDev D = eng_.make_job(J);
-      D.out = dev_out;
-      D.starts = dev_starts;
-      const unsigned long long b0 = published_items_;
-      if (dev_starts)
-        cuda_check(cudaMemcpyAsync(dev_starts, r->a.data(), J.n_starts * 4, cudaMemcpyHostToDevice, cstream_),
-                   "starts H2D");
-      cuda_check(cudaMemcpyAsync(jobs_.as<WalkJobDev>() + slot, &D, sizeof D, cudaMemcpyHostToDevice, cstream_),
-                 "job H2D");
-      cuda_check(cudaMemcpyAsync(base_.as<unsigned long long>() + slot, &b0, 8, cudaMemcpyHostToDevice, cstream_),
+      // Publish sources go through the pinned staging ring so the copies are
+      // asynchronous; the ring restarts once the publish stream has drained.
+      const size_t need_pin = sizeof(WalkJobDev) + 64 + (dev_starts ? J.n_starts * 4 : 0);
+      if (pin_head_ + need_pin > kPinBytes) {
+        cuda_check(cudaStreamSynchronize(cstream_), "staging wrap");
+        pin_head_ = 0;
+      }
+      WalkJobDev* hD = reinterpret_cast<WalkJobDev*>(pin_ + pin_head_);
+      *hD = eng_.make_job(J);
+      hD->out = dev_out;
+      hD->starts = dev_starts;
+      hD->seq = seq;
+      pin_head_ += (sizeof(WalkJobDev) + 63) & ~(size_t)63;
+      if (dev_starts) {
+        uint32_t* hs = reinterpret_cast<uint32_t*>(pin_ + pin_head_);
+        std::memcpy(hs, r->a.data(), J.n_starts * 4);
+        pin_head_ += (J.n_starts * 4 + 63) & ~(size_t)63;
+        cuda_check(cudaMemcpyAsync(dev_starts, hs, J.n_starts * 4, cudaMemcpyHostToDevice, cstream_), "starts H2D");
+      }
+      cuda_check(cudaMemcpyAsync(jobs_.as<WalkJobDev>() + slot, hD, sizeof(WalkJobDev), cudaMemcpyHostToDevice,
+                                 cstream_),
                  "job H2D");
       cuda_check(cudaMemsetAsync(&state_.as<ServeDevState>()->done[slot], 0, 4, cstream_), "job reset");
-      cuda_check(cudaStreamSynchronize(cstream_), "job publish");
       done_seq_[slot] = 0;
-      published_items_ += J.n_starts;
       ++published_jobs_;
-      std::atomic_thread_fence(std::memory_order_seq_cst);
-      ctl_->published_items = published_items_;
-      ctl_->published_jobs = published_jobs_;
-      std::atomic_thread_fence(std::memory_order_seq_cst);
+      ctl_.published_jobs = published_jobs_;
+      push_ctl();  // ordered after the descriptor copies on the same stream
       inflight_.push_back(InFlight{r->ticket, seq, off, ob + sb, dev_out, J.out, out_bytes});
+      inflight_.back().admit_ns = t_adm;
       {
         std::lock_guard<std::mutex> lk(mu_);
         tickets_[r->ticket].version = version_;
+        m_.queue_ns += t_adm - tickets_[r->ticket].submit_ns;
         queue_.pop_front();
       }
       launch_kernel();
       progress = true;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        m_.admit_ns += now_ns() - t_adm;
+        m_.max_inflight = std::max<uint64_t>(m_.max_inflight, inflight_.size());
+      }
     } else {
       // An update waits for every walk admitted before it, then commits.
-      if (!inflight_.empty() || oldest_ != published_jobs_) {
-        ctl_->drain = 1;
-        break;
+      if (!ctl_.drain) {
+        ctl_.drain = 1;
+        push_ctl();
+        drain_since_ = now_ns();
+        drain_retired_ = 0;
       }
-      ctl_->drain = 1;
+      if (!inflight_.empty() || oldest_ != published_jobs_) break;
+      if (!drain_retired_) drain_retired_ = now_ns();
       if (kernel_running()) break;
+      const uint64_t t_upd = now_ns();
       int st = BINGO_OK;
       try {
         const uint64_t k = r->a.size();
@@ -452,7 +548,14 @@ bool Server::step() {
         st = e.status;
       }
       ++version_;
-      ctl_->drain = 0;
+      ctl_.drain = 0;
+      push_ctl();
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        m_.update_ns += now_ns() - t_upd;
+        m_.drain_wait_ns += t_upd - drain_since_;
+        m_.drain_inflight_ns += drain_retired_ - drain_since_;
+      }
       const uint64_t t = r->ticket;
       {
         std::lock_guard<std::mutex> lk(mu_);
@@ -461,6 +564,11 @@ bool Server::step() {
       finish_ticket(t, st, version_);
       progress = true;
     }
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    m_.complete_ns += t_completed - t_begin;
+    ++m_.scheduler_passes;
   }
   // Keep a kernel alive while admitted walks are unfinished.
   if (!inflight_.empty() && !kernel_running()) {
@@ -505,8 +613,36 @@ void Server::loop() {
       }
     }
   }
-  ctl_->stop = 1;
+  ctl_.stop = 1;
+  try {
+    push_ctl();
+  } catch (...) {
+  }
+  cudaStreamSynchronize(cstream_);
   cudaStreamSynchronize(kstream_);
+}
+
+// Copies the host shadow of the control block to the device (stream order
+// keeps it after the job descriptors it exposes; pageable source, so the
+// shadow may change once the call returns).
+void Server::push_ctl() {
+  if (pin_head_ + 64 > kPinBytes) {
+    cuda_check(cudaStreamSynchronize(cstream_), "staging wrap");
+    pin_head_ = 0;
+  }
+  void* h = pin_ + pin_head_;
+  std::memcpy(h, (const void*)&ctl_, sizeof ctl_);
+  pin_head_ += 64;
+  cuda_check(cudaMemcpyAsync(d_ctl_, h, sizeof ctl_, cudaMemcpyHostToDevice, cstream_), "serve control");
+}
+
+void Server::metrics(bingo_serve_metrics* out) {
+  std::lock_guard<std::mutex> lk(mu_);
+  *out = m_;
+  out->submitted = next_ticket_;
+  uint64_t c = 0;
+  for (auto& kv : tickets_) c += kv.second.done;
+  out->completed = c;
 }
 
 void Server::stats(uint64_t* completed, uint64_t* version) {

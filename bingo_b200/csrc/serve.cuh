@@ -9,6 +9,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/bingo.h"
 #include "common.cuh"
@@ -17,20 +18,25 @@
 namespace bingo {
 
 constexpr uint32_t kServeMaxJobs = 4096;  // job ring capacity (power of two)
+constexpr size_t kPinBytes = 64u << 20;    // pinned staging ring for publish copies
 
-// Control block in mapped pinned host memory: written by the host, polled
-// by the serving kernel.
+// Control block in device memory: written by the host (stream-ordered
+// copies), polled by the serving kernel.
 struct ServeCtl {
-  volatile unsigned long long published_items;  // walk items [0, published_items) are claimable
-  volatile uint32_t published_jobs;             // job sequence numbers [0, published_jobs) are visible
-  volatile uint32_t oldest_job;                 // lowest sequence number not yet retired
-  volatile uint32_t drain;                      // exit once every published item is finished
-  volatile uint32_t stop;                       // exit now
+  volatile uint32_t published_jobs;  // job sequence numbers [0, published_jobs) are visible
+  volatile uint32_t drain;           // exit once every published walk is claimed and finished
+  volatile uint32_t stop;            // exit now
+  uint32_t pad;
 };
 
-// Device-resident serving state.
+// Device-resident serving state. Walks are claimed per job: claim[slot]
+// holds (job sequence number << 32) | walks handed out, opened by the warp
+// that moves head_job onto that job, and taken 32 at a time by fetch-add
+// (a tag that does not match the job asked for means "not open yet").
 struct ServeDevState {
-  unsigned long long next_item;  // next unclaimed walk item
+  uint32_t head_job;  // lowest job sequence number that may still have unclaimed walks
+  uint32_t closing;   // set by the first warp that exits idle; every warp then exits (reset per launch)
+  unsigned long long claim[kServeMaxJobs];
   uint32_t done[kServeMaxJobs];  // finished walks per ring slot
 };
 
@@ -44,6 +50,7 @@ class Server {
   bool poll(uint64_t ticket, bingo_serve_status* out);
   bool wait(uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out);
   void stats(uint64_t* completed, uint64_t* version);
+  void metrics(bingo_serve_metrics* out);
 
  private:
   struct Request;
@@ -65,17 +72,21 @@ class Server {
   void release_region(size_t off);
   bool kernel_running();
   void launch_kernel();
+  void push_ctl();
   bool step();
   void loop();
 
   Engine& eng_;
   bingo_serve_config cfg_;
-  cudaStream_t kstream_ = nullptr, cstream_ = nullptr;
-  ServeCtl* ctl_ = nullptr;
+  cudaStream_t kstream_ = nullptr, cstream_ = nullptr, rstream_ = nullptr;  // kernel, publish, results
+  char* pin_ = nullptr;  // pinned staging ring
+  size_t pin_head_ = 0;
+  std::vector<cudaEvent_t> event_pool_;
+  ServeCtl ctl_;             // host shadow
   ServeCtl* d_ctl_ = nullptr;
   volatile unsigned long long* done_seq_ = nullptr;
   unsigned long long* d_done_seq_ = nullptr;
-  DevBuf jobs_, base_, state_, budget_;
+  DevBuf jobs_, state_, budget_, ctlbuf_;
   bool launched_ = false;
 
   // scheduler-thread state
@@ -84,8 +95,9 @@ class Server {
   std::deque<Region> regions_;
   size_t head_ = 0, tail_ = 0;
   uint32_t published_jobs_ = 0, oldest_ = 0;
-  unsigned long long published_items_ = 0;
   uint64_t version_ = 0;
+  bingo_serve_metrics m_{};  // scheduler counters (guarded by mu_ when read)
+  uint64_t drain_since_ = 0, drain_retired_ = 0;
 
   // shared with submitters
   std::mutex mu_;

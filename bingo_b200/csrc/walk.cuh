@@ -28,7 +28,7 @@ struct WalkJobDev {
   uint32_t job;
   uint32_t k0, k1;  // Philox key (seed)
   uint32_t flags;
-  uint32_t pad;
+  uint32_t seq;  // serving ring: the job's sequence number (0 elsewhere)
   unsigned long long thr_ret, thr_in, thr_out, thr_stop;  // 33-bit acceptance thresholds
   double ret_excess;  // node2vec: (1/p) / max(1, 1/q) - 1 when positive, else 0
   int32_t* out;

@@ -14,8 +14,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import (BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeStatus, BingoStats, BingoWalkJob,
-                   lib)
+from ._lib import (BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeMetrics, BingoServeStatus,
+                   BingoStats, BingoWalkJob, lib)
 
 DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
@@ -257,7 +257,7 @@ class Graph:
     @staticmethod
     def _status(s: BingoServeStatus) -> dict:
         return {"done": bool(s.done), "status": s.status, "kind": s.kind, "version": s.version,
-                "latency_ns": s.latency_ns}
+                "latency_ns": s.latency_ns, "ready_ns": s.ready_ns}
 
     def serve_poll(self, ticket: int) -> dict:
         s = BingoServeStatus()
@@ -270,6 +270,11 @@ class Graph:
         self._check(self._L.bingo_serve_wait(self._h, ticket, timeout_us, ctypes.byref(s)))
         self._serve_keep.pop(ticket, None)
         return self._status(s)
+
+    def serve_metrics(self) -> dict:
+        m = BingoServeMetrics()
+        self._check(self._L.bingo_serve_get_metrics(self._h, ctypes.byref(m)))
+        return {f: getattr(m, f) for f, _ in BingoServeMetrics._fields_}
 
     def serve_stop(self):
         self._check(self._L.bingo_serve_stop(self._h))

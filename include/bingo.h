@@ -213,6 +213,7 @@ typedef struct bingo_serve_status {
   int32_t reserved0;
   uint64_t version;    /* updates applied before this request (walks) / including it (updates) */
   uint64_t latency_ns; /* submit to result ready */
+  uint64_t ready_ns;   /* when the result became ready, CLOCK_MONOTONIC nanoseconds */
 } bingo_serve_status;
 
 int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg);
@@ -224,6 +225,20 @@ int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, 
 int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);
 /* Waits at most timeout_us; returns BINGO_ERR_TIMEOUT if the ticket is not done. */
 int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out);
+/* Scheduler counters since bingo_serve_start (times in ns of scheduler-thread wall time). */
+typedef struct bingo_serve_metrics {
+  uint64_t submitted, completed;
+  uint64_t walk_kernel_launches; /* serving-loop launches (relaunched after idle exits and updates) */
+  uint64_t scheduler_passes;
+  uint64_t admit_ns, complete_ns, update_ns, drain_wait_ns;
+  uint64_t max_inflight;         /* most walk queries in flight at once */
+  uint64_t queue_ns;             /* sum over walk queries of submit -> admission */
+  uint64_t device_ns;            /* sum over walk queries of admission -> last walk finished (host-observed) */
+  uint64_t copy_ns;              /* sum over walk queries of last walk finished -> result in caller memory */
+  uint64_t drain_inflight_ns;    /* part of drain_wait_ns until earlier queries retired */
+} bingo_serve_metrics;
+int bingo_serve_get_metrics(bingo_handle* h, bingo_serve_metrics* out);
+
 /* Finishes every submitted request, stops the walk loop, returns the handle to normal use. */
 int bingo_serve_stop(bingo_handle* h);
 
