@@ -411,6 +411,26 @@ def run_served(args):
                 outs.append(None)
         return outs
 
+    # Untimed warm-up of both forms (module loads, first allocations, update
+    # scratch), on a copy of the graph that each rate reloads anyway.
+    prepare(0)
+    wu = make_trace(np.random.default_rng(S_SEED + 9), n, walkable, gen.UpdateGen(n, src, dst, seed=S_SEED + 8),
+                    24, 1000.0, 0.25)
+    wouts = outputs(wu)
+    g.serve_start(output_budget_bytes=args.serve_budget << 20, max_update_batch=1 << 20, idle_timeout_us=3000)
+    wt = [g.submit_walk(app=x[0], length=WALK_LEN, starts=x[1], seed=7, job_id=x[2], stop_prob=0.15, out=o)[0]
+          if k == "walk" else g.submit_update(k, *x)[0] for (k, _, x), o in zip(wu, wouts)]
+    for t in wt:
+        g.serve_wait(t, timeout_us=600_000_000)
+    g.serve_stop()
+    for (k, _, x), o in zip(wu, wouts):
+        if k == "walk":
+            g.walk(app=x[0], length=WALK_LEN, starts=x[1], seed=7, job_id=x[2], stop_prob=0.15, out=o)
+        elif k == "insert":
+            g.insert_batch(*x, return_slots=False)
+        else:
+            g.delete_batch(*x)
+
     results = []
     for ri, (rate, tr) in enumerate(zip(rates, traces)):
         outs = outputs(tr)

@@ -107,6 +107,7 @@ SIGNATURES = {
     "bingo_load_edges": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_uint32]),
     "bingo_insert_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
     "bingo_delete_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
+    "bingo_delete_pairs": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "bingo_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32, c_uint32]),
     "bingo_walk_noalloc": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32]),
     "bingo_run": (c_int, [c_void_p, POINTER(BingoOp), c_uint32, c_uint32]),

@@ -115,6 +115,10 @@ int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot,
   return guarded(h, [&](bingo::Engine& e) { e.erase(u, slot, k); });
 }
 
+int bingo_delete_pairs(bingo_handle* h, const uint32_t* u, const uint32_t* v, uint64_t k) {
+  return guarded(h, [&](bingo::Engine& e) { e.erase_pairs(u, v, k); });
+}
+
 int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   return guarded(h, [&](bingo::Engine& e) { e.walk(jobs, n_jobs, mode); });
 }

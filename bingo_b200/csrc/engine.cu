@@ -169,6 +169,53 @@ __global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint
   }
 }
 
+// Delete by pair, step 1: 64-bit sort keys (u << 32) | v.
+__global__ void k_pair_keys(const uint32_t* u, const uint32_t* v, unsigned long long k, unsigned long long* key) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    key[i] = ((unsigned long long)u[i] << 32) | v[i];
+}
+
+// Step 2: run heads of equal pairs in the sorted keys.
+__global__ void k_pair_heads(const unsigned long long* key, unsigned long long k, uint8_t* head) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    head[i] = i == 0 || key[i] != key[i - 1];
+}
+
+// Step 3: one warp per run of equal pairs (u, v), in batch order (the sort is
+// stable): its r-th member takes the r-th lowest live slot of u whose
+// neighbour is v, or ~0 (an absent slot, skipped and counted by the delete)
+// when u has fewer such slots. Slots are scanned 32 at a time with one
+// 16-byte load per lane.
+__global__ void __launch_bounds__(kBlock) k_pair_slots(StoreView S, const unsigned long long* key,
+                                                       const uint32_t* perm, const uint32_t* seg,
+                                                       const uint32_t* nseg, unsigned long long k,
+                                                       const uint32_t* ctl, uint32_t* slot_out) {
+  if (*ctl) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * blockDim.x / 32;
+  const uint32_t nS = *nseg;
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
+    uint32_t b, e;
+    seg_bounds(seg, nS, s, k, &b, &e);
+    const uint32_t u = (uint32_t)(key[b] >> 32), v = (uint32_t)key[b];
+    const uint32_t want = e - b;
+    const VertexMeta M = S.meta[u];
+    uint32_t got = 0;
+    for (uint32_t c = 0; c < M.ecnt && got < want; c += 32) {
+      const uint32_t i = c + lane;
+      EdgeRec r{0, 0, 0, 0};
+      if (i < M.ecnt) r = S.edges[M.eoff + i];
+      const uint32_t hit = __ballot_sync(kFull, i < M.ecnt && r.v == v && r.w != 0);
+      const uint32_t rank = got + __popc(hit & lanemask_lt());
+      if (((hit >> lane) & 1) && rank < want) slot_out[perm[b + rank]] = i;
+      got += __popc(hit);
+    }
+    for (uint32_t r = got + lane; r < want; r += 32) slot_out[perm[b + r]] = 0xffffffffu;
+  }
+}
+
 // Persistent walk kernel with per-lane refill. Each warp owns a range of
 // walk items and hands them to idle lanes; when the range runs out it pulls
 // the next kWalkChunk items from one device counter (reset by the host before
@@ -465,7 +512,7 @@ Engine::~Engine() {
   prog_jobs_.release(), prog_prefix_.release(), prog_queue_.release();
   DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
                     &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
-                    &prefix_, &queue_, &wstart_, &wout_};
+                    &prefix_, &queue_, &wstart_, &wout_, &pair_key_, &pair_key_s_, &pair_slot_};
   for (DevBuf* b : bufs) b->release();
   for (auto& a : arena_) a.release();
   if (d_err_) cudaFree(d_err_);
@@ -824,6 +871,60 @@ void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   cuda_check(cudaGetLastError(), "apply delete");
   ++launches_;
   finish_call();
+}
+
+// Delete by (u, v) pair. No reference counterpart (the reference deletes by
+// (u, slot), include/operation.cuh:215): the r-th occurrence of a pair in
+// the batch deletes the r-th lowest live slot of u whose neighbour is v;
+// pairs without such a slot are skipped and reported like deletes of absent
+// slots. The translated (u, slot) batch then takes the slot-delete path, so
+// the swap-remove order is the batch order.
+void Engine::erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k) {
+  require_loaded();
+  if (k == 0) return;
+  if (!u || !v) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null delete array");
+  if (k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 deletes in one batch");
+  if (!is_device_ptr(u)) host_check_ids(u, k, n_, "vertex");
+  if (!is_device_ptr(v)) host_check_ids(v, k, n_, "vertex");
+  ensure_batch_scratch(k);
+  pair_key_.ensure(k * 8, "scratch");
+  pair_key_s_.ensure(k * 8, "scratch");
+  pair_slot_.ensure(k * 4, "scratch");
+  int end_bit = 33;
+  while (end_bit < 64 && (1ull << (end_bit - 32)) < n_) ++end_bit;
+  size_t t_sort = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                  (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)k, 0, end_bit, stream_);
+  cub_tmp_.ensure(t_sort, "scratch");
+  const uint32_t* du = stage(u, k, in_a_, "stage u");
+  const uint32_t* dv = stage(v, k, in_b_, "stage v");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, dv, nullptr, k, n_, ctl_.as<uint32_t>(), d_err_);
+  k_pair_keys<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, dv, k, pair_key_.as<unsigned long long>());
+  cuda_check(cudaGetLastError(), "pair keys");
+  launches_ += 2;
+  size_t tb = cub_tmp_.bytes;
+  cuda_check(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tb, pair_key_.as<unsigned long long>(),
+                                             pair_key_s_.as<unsigned long long>(), iota_.as<uint32_t>(),
+                                             perm_.as<uint32_t>(), (int)k, 0, end_bit, stream_),
+             "pair sort");
+  k_pair_heads<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(pair_key_s_.as<unsigned long long>(), k,
+                                                                  head_.as<uint8_t>());
+  cuda_check(cudaGetLastError(), "pair heads");
+  ++launches_;
+  tb = cub_tmp_.bytes;
+  cuda_check(cub::DeviceSelect::Flagged(cub_tmp_.p, tb, iota_.as<uint32_t>(), head_.as<uint8_t>(),
+                                        seg_.as<uint32_t>(), nseg_.as<uint32_t>(), (int)k, stream_),
+             "pair runs");
+  // Absent until matched: a batch rejected by validation deletes nothing.
+  cuda_check(cudaMemsetAsync(pair_slot_.p, 0xff, k * 4, stream_), "pair slots");
+  const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
+  k_pair_slots<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+      view(), pair_key_s_.as<unsigned long long>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
+      nseg_.as<uint32_t>(), k, ctl_.as<uint32_t>(), pair_slot_.as<uint32_t>());
+  cuda_check(cudaGetLastError(), "pair slots");
+  ++launches_;
+  erase(du, pair_slot_.as<uint32_t>(), k);
 }
 
 void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {

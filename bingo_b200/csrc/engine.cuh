@@ -47,6 +47,7 @@ class Engine {
   void load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n);
   void insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
   void erase(const uint32_t* u, const uint32_t* slot, uint64_t k);
+  void erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k);
   void walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
   void walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs);
   void run(const bingo_op* ops, uint32_t n_ops, uint32_t flags);
@@ -97,6 +98,7 @@ class Engine {
   // per-batch scratch
   DevBuf in_a_, in_b_, in_c_, key_s_, perm_, iota_, sa_, sb_, head_, seg_, nseg_, need_, scan_, base_, ctl_,
       slots_, cub_tmp_;
+  DevBuf pair_key_, pair_key_s_, pair_slot_;  // delete-by-pair translation
   uint64_t iota_n_ = 0;
   // walk scratch
   DevBuf jobs_, prefix_, queue_, wstart_, wout_;

@@ -141,6 +141,13 @@ class Graph:
         psl, ksl = _u32(slot)
         self._check(self._L.bingo_delete_batch(self._h, pu, psl, k))
 
+    def delete_pairs(self, u, v):
+        """Delete edges by (u, v): the r-th repeat of a pair takes the r-th lowest live slot (bingo_delete_pairs)."""
+        k = len(u) if not hasattr(u, "numel") else u.numel()
+        pu, ku = _u32(u)
+        pv, kv = _u32(v)
+        self._check(self._L.bingo_delete_pairs(self._h, pu, pv, k))
+
     @staticmethod
     def _job_array(jobs: Sequence[WalkJob], keep: list):
         arr = (BingoWalkJob * len(jobs))()

@@ -128,6 +128,14 @@ int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst
  * call returns BINGO_ERR_INVALID_SLOT after applying the rest. */
 int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot, uint64_t k);
 
+/* Delete by (u, v) pair; no reference counterpart (the reference deletes by
+ * slot only, include/operation.cuh:215). The r-th occurrence of a pair in the
+ * batch deletes the r-th lowest live slot of u whose neighbour is v; the
+ * translated (u, slot) batch then applies exactly as bingo_delete_batch.
+ * Pairs with no such slot are skipped and the call returns
+ * BINGO_ERR_INVALID_SLOT after applying the rest. */
+int bingo_delete_pairs(bingo_handle* h, const uint32_t* u, const uint32_t* v, uint64_t k);
+
 /* Replaces the walk kernels deepwalkKernel / node2vecKernel / pprKernel /
  * samplingKernel<<<BLKSZ, THDSZ>>>(gId, pId, n, NodeData*, int* rwD, PIECESIZE, seed)
  * (include/operation.cuh:252, :281, :336, :407) and the randomWalk driver

@@ -36,6 +36,7 @@
 #include <cstdint>
 #include <cstring>
 #include <unordered_map>
+#include <map>
 #include <vector>
 
 namespace oracle {
@@ -328,6 +329,22 @@ struct ExactGraph {
       rebuild_alias(x);
     }
     return bad;
+  }
+
+  // Delete by (u, v): the r-th occurrence of a pair in the batch takes the
+  // r-th lowest live slot of u with neighbour v (~0 when there is none); the
+  // slot list then goes through erase(). Returns erase()'s rejected count.
+  uint64_t erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k, uint32_t* slots_out = nullptr) {
+    std::vector<uint32_t> slot(k, 0xffffffffu);
+    std::map<std::pair<uint32_t, uint32_t>, uint32_t> next;  // first slot not yet examined per pair
+    for (uint64_t i = 0; i < k; ++i) {
+      const Vertex& X = vx[u[i]];
+      uint32_t& c = next[{u[i], v[i]}];
+      while (c < X.ev.size() && !(X.ev[c] == v[i] && X.ew[c] != 0)) ++c;
+      if (c < X.ev.size()) slot[i] = c++;
+    }
+    if (slots_out) std::copy(slot.begin(), slot.end(), slots_out);
+    return erase(u, slot.data(), k);
   }
 
   // One weighted neighbour draw from the alias table, then a uniform member.

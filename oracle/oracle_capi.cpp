@@ -43,6 +43,9 @@ void orc_insert(void* g, const uint32_t* src, const uint32_t* dst, const uint32_
 uint64_t orc_delete(void* g, const uint32_t* u, const uint32_t* slot, uint64_t k) {
   return ((ExactGraph*)g)->erase(u, slot, k);
 }
+uint64_t orc_delete_pairs(void* g, const uint32_t* u, const uint32_t* v, uint64_t k, uint32_t* slots_out) {
+  return ((ExactGraph*)g)->erase_pairs(u, v, k, slots_out);
+}
 void orc_walk(void* g, int app, uint32_t L, const uint32_t* starts, uint64_t n_starts, uint64_t seed, uint32_t job,
               double p, double q, double stop, uint32_t flags, int32_t* out) {
   ((const ExactGraph*)g)->walk(app, L, starts, n_starts, seed, job, p, q, stop, flags, out);

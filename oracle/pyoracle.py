@@ -37,6 +37,7 @@ def lib():
             "orc_load": (None, [vp, vp, vp, vp, c_uint64]),
             "orc_insert": (None, [vp, vp, vp, vp, c_uint64, vp]),
             "orc_delete": (c_uint64, [vp, vp, vp, c_uint64]),
+            "orc_delete_pairs": (c_uint64, [vp, vp, vp, c_uint64, vp]),
             "orc_walk": (None, [vp, c_int, c_uint32, vp, c_uint64, c_uint64, c_uint32, c_double, c_double,
                                 c_double, c_uint32, vp]),
             "orc_has_edge": (c_int, [vp, c_uint32, c_uint32]),
@@ -118,6 +119,13 @@ class ExactGraph:
     def delete(self, u, slot):
         uu, ss = _u32(u), _u32(slot)
         return lib().orc_delete(self._g, _p(uu), _p(ss), len(uu))
+
+    def delete_pairs(self, u, v):
+        """Returns (rejected count, translated slot per pair)."""
+        uu, vv = _u32(u), _u32(v)
+        out = np.zeros(len(uu), np.uint32)
+        bad = lib().orc_delete_pairs(self._g, _p(uu), _p(vv), len(uu), _p(out))
+        return bad, out
 
     def walk(self, app, length, starts, seed=0, job_id=0, p=0.5, q=2.0, stop=0.0125, flags=0):
         st = _u32(starts)

@@ -196,3 +196,19 @@ def test_reference_config1_digests():
     for i, (mine, want) in enumerate(zip(dumps, rec["dumps"])):
         for k in po.REF_DUMP_FIELDS:
             assert dig(mine[k]) == want[k], f"config1 dump {i} field {k}"
+
+
+def test_oracle_delete_pairs_rank_semantics():
+    """r-th repeat of (u, v) takes the r-th lowest live slot; extra repeats and
+    absent pairs are rejected without touching the graph."""
+    ex = po.ExactGraph(4)
+    src = np.array([0, 0, 0, 0, 1], np.uint32)
+    dst = np.array([1, 2, 1, 1, 2], np.uint32)
+    w = np.array([3, 5, 7, 9, 1], np.uint32)
+    ex.load(src, dst, w)
+    ex.delete(np.array([0], np.uint32), np.array([2], np.uint32))  # slot 2 (0->1) is now a tombstone
+    bad, slots = ex.delete_pairs(np.array([0, 1, 0, 0, 2], np.uint32), np.array([1, 2, 1, 1, 3], np.uint32))
+    assert list(slots) == [0, 0, 3, 0xFFFFFFFF, 0xFFFFFFFF]
+    assert bad == 2
+    d = ex.dump()
+    assert d["live"][0] == 1 and d["live"][1] == 0
