@@ -77,6 +77,26 @@ class BingoServeStatus(ctypes.Structure):
     ]
 
 
+TUNING_FIELDS = ("walk_chunk", "walk_blocks_per_sm", "walk_split", "walk_order", "update_chunk",
+                 "apply_blocks_per_sm")
+
+
+class BingoTuning(ctypes.Structure):
+    _fields_ = [(f, c_uint32) for f in TUNING_FIELDS] + [("reserved", c_uint32 * 2)]
+
+
+class BingoTuneRequest(ctypes.Structure):
+    _fields_ = [("jobs", c_void_p), ("n_jobs", c_uint32), ("repeats", c_uint32), ("ins_src", c_void_p),
+                ("ins_dst", c_void_p), ("ins_w", c_void_p), ("n_ins", c_uint64), ("del_u", c_void_p),
+                ("del_slot", c_void_p), ("n_del", c_uint64)]
+
+
+class BingoTuneReport(ctypes.Structure):
+    _fields_ = [("best", BingoTuning), ("walk_ms_start", ctypes.c_double), ("walk_ms_best", ctypes.c_double),
+                ("update_ms_start", ctypes.c_double), ("update_ms_best", ctypes.c_double),
+                ("candidates", c_uint32), ("reserved0", c_uint32)]
+
+
 class BingoServeMetrics(ctypes.Structure):
     _fields_ = [(f, c_uint64) for f in ("submitted", "completed", "walk_kernel_launches", "scheduler_passes",
                                          "admit_ns", "complete_ns", "update_ns", "drain_wait_ns", "max_inflight",
@@ -120,6 +140,9 @@ SIGNATURES = {
     "bingo_serve_wait": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(BingoServeStatus)]),
     "bingo_serve_stop": (c_int, [c_void_p]),
     "bingo_serve_get_metrics": (c_int, [c_void_p, POINTER(BingoServeMetrics)]),
+    "bingo_get_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
+    "bingo_set_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
+    "bingo_autotune": (c_int, [c_void_p, POINTER(BingoTuneRequest), POINTER(BingoTuneReport)]),
     "bingo_set_stream": (c_int, [c_void_p, c_void_p]),
     "bingo_get_stats": (c_int, [c_void_p, POINTER(BingoStats)]),
     "bingo_dump_sizes": (c_int, [c_void_p, POINTER(c_uint64)]),

@@ -146,6 +146,42 @@ int bingo_get_stats(bingo_handle* h, bingo_stats* out) {
   return guarded(h, [&](bingo::Engine& e) { e.stats(out); }, true);
 }
 
+int bingo_get_tuning(bingo_handle* h, bingo_tuning* out) {
+  if (!out) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(
+      h,
+      [&](bingo::Engine& e) {
+        const bingo::Tuning& t = e.tuning();
+        *out = bingo_tuning{};
+        out->walk_chunk = t.walk_chunk;
+        out->walk_blocks_per_sm = t.walk_blocks_per_sm;
+        out->walk_split = t.walk_split;
+        out->walk_order = t.walk_order;
+        out->update_chunk = t.update_chunk;
+        out->apply_blocks_per_sm = t.apply_blocks_per_sm;
+      },
+      true);
+}
+
+int bingo_set_tuning(bingo_handle* h, const bingo_tuning* in) {
+  if (!in) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) {
+    bingo::Tuning t;
+    t.walk_chunk = in->walk_chunk;
+    t.walk_blocks_per_sm = in->walk_blocks_per_sm;
+    t.walk_split = in->walk_split;
+    t.walk_order = in->walk_order;
+    t.update_chunk = in->update_chunk;
+    t.apply_blocks_per_sm = in->apply_blocks_per_sm;
+    e.set_tuning(t);
+  });
+}
+
+int bingo_autotune(bingo_handle* h, const bingo_tune_request* req, bingo_tune_report* out) {
+  if (!req) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) { e.autotune(*req, out); });
+}
+
 int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg) {
   bingo_serve_config c{};
   if (cfg) c = *cfg;

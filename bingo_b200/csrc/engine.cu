@@ -60,7 +60,7 @@ __global__ void k_validate(const uint32_t* a, const uint32_t* b, const uint32_t*
   uint32_t bits = 0;
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
        i += (unsigned long long)gridDim.x * blockDim.x) {
-    if (a[i] >= n || (b && b[i] >= n)) bits |= E_RANGE;
+    if ((a && a[i] >= n) || (b && b[i] >= n)) bits |= E_RANGE;
     if (w && w[i] == 0u) bits |= E_ZERO_WEIGHT;
   }
   bits = __reduce_or_sync(kFull, bits);
@@ -218,12 +218,12 @@ __global__ void __launch_bounds__(kBlock) k_pair_slots(StoreView S, const unsign
 
 // Persistent walk kernel with per-lane refill. Each warp owns a range of
 // walk items and hands them to idle lanes; when the range runs out it pulls
-// the next kWalkChunk items from one device counter (reset by the host before
+// the next `chunk` items from one device counter (reset by the host before
 // launch). MULTI = false: every item is a walk of the single job J0.
 // MULTI = true: items index the concatenated jobs of a device job table
 // (prefix = running walk counts) and each lane follows its own job; APP >= 0
 // when every job of the table has that app, APP < 0 for a mixed table.
-constexpr uint32_t kWalkChunk = 32;
+// `chunk` (walks per warp refill) is a tuning knob (Tuning::walk_chunk).
 static_assert(kBlock % 32 == 0, "whole warps");
 
 // Resident 256-thread blocks per SM each walk variant is compiled for
@@ -240,7 +240,7 @@ constexpr int walk_min_blocks(int app, bool multi) {
 template <int APP, bool MULTI>
 __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP, MULTI))
     k_walk(WalkView W, WalkJobDev J0, const WalkJobDev* __restrict__ jobs, const uint32_t* __restrict__ prefix,
-           uint32_t n_jobs, uint32_t total, uint32_t* queue) {
+           uint32_t n_jobs, uint32_t total, uint32_t* queue, uint32_t chunk) {
   __shared__ __align__(16) int32_t obuf[kBlock][8];
   const int lane = threadIdx.x & 31;
   LaneWalk s;
@@ -252,14 +252,14 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP, MULTI))
     while (idle && !drained) {
       if (wb >= we) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(queue, kWalkChunk);
+        if (lane == 0) base = atomicAdd(queue, chunk);
         base = __shfl_sync(kFull, base, 0);
         if (base >= total) {
           drained = true;
           break;
         }
         wb = base;
-        we = min(base + kWalkChunk, total);
+        we = base + min(chunk, total - base);
       }
       const uint32_t take = min((uint32_t)__popc(idle), we - wb);
       const uint32_t rank = __popc(idle & lanemask_lt());
@@ -325,30 +325,40 @@ unsigned walk_blocks_per_sm() {
   return (unsigned)b;
 }
 
+// Blocks per SM for a walk launch: the tuned figure capped by occupancy
+// (0 = occupancy).
+unsigned walk_bps(unsigned occ, const Tuning& t) {
+  return t.walk_blocks_per_sm ? std::max(1u, std::min(occ, t.walk_blocks_per_sm)) : occ;
+}
+
 // Launches the persistent walk kernel for a device job table whose jobs all
 // have app `app` (or any app when app < 0).
 void launch_walk_table(cudaStream_t st, int app, const WalkView& W, const WalkJobDev& J0, const WalkJobDev* jobs,
-                       const uint32_t* prefix, uint32_t n_jobs, uint32_t total, uint32_t* queue) {
+                       const uint32_t* prefix, uint32_t n_jobs, uint32_t total, uint32_t* queue, const Tuning& t) {
+  const uint32_t c = t.walk_chunk;
   switch (app) {
     case APP_DEEPWALK:
-      k_walk<APP_DEEPWALK, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_DEEPWALK, true>()), kBlock, 0,
-                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      k_walk<APP_DEEPWALK, true>
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_DEEPWALK, true>(), t)), kBlock, 0, st>>>(
+              W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_NODE2VEC:
-      k_walk<APP_NODE2VEC, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_NODE2VEC, true>()), kBlock, 0,
-                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      k_walk<APP_NODE2VEC, true>
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_NODE2VEC, true>(), t)), kBlock, 0, st>>>(
+              W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_PPR:
-      k_walk<APP_PPR, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_PPR, true>()), kBlock, 0, st>>>(
-          W, J0, jobs, prefix, n_jobs, total, queue);
+      k_walk<APP_PPR, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_PPR, true>(), t)), kBlock, 0, st>>>(
+          W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_SAMPLING:
-      k_walk<APP_SAMPLING, true><<<grid_for(total, kBlock, walk_blocks_per_sm<APP_SAMPLING, true>()), kBlock, 0,
-                                   st>>>(W, J0, jobs, prefix, n_jobs, total, queue);
+      k_walk<APP_SAMPLING, true>
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_SAMPLING, true>(), t)), kBlock, 0, st>>>(
+              W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     default:
-      k_walk<-1, true><<<grid_for(total, kBlock, walk_blocks_per_sm<-1, true>()), kBlock, 0, st>>>(
-          W, J0, jobs, prefix, n_jobs, total, queue);
+      k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), t)), kBlock, 0, st>>>(
+          W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
   }
   cuda_check(cudaGetLastError(), "walk launch");
@@ -363,31 +373,24 @@ struct WalkGroup {
   uint32_t total;     // walks
 };
 
-bool walk_split_by_app() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = std::getenv("BINGO_WALK_SPLIT");
-    v = (e && std::strcmp(e, "1") == 0) ? 1 : 0;  // one mixed launch measured faster
-  }
-  return v == 1;
-}
-
 double walk_cost(const WalkJobDev& J);
 
 // Appends the jobs `in` to (table, prefix) as one group per app present
 // (or one mixed group), each ordered by expected walk cost, most expensive
-// first, so the longest walks start earliest. Outputs are per job, so the
-// order does not change any result.
-void build_walk_groups(const WalkJobDev* in, uint32_t n, bool split, std::vector<WalkJobDev>& table,
-                       std::vector<uint32_t>& prefix, std::vector<WalkGroup>& groups) {
+// first, so the longest walks start earliest (longest_first = false keeps
+// the given order). Outputs are per job, so the order does not change any
+// result.
+void build_walk_groups(const WalkJobDev* in, uint32_t n, bool split, bool longest_first,
+                       std::vector<WalkJobDev>& table, std::vector<uint32_t>& prefix, std::vector<WalkGroup>& groups) {
   std::vector<uint32_t> idx;
   for (int app = split ? 0 : -1; app <= (split ? 3 : -1); ++app) {
     idx.clear();
     for (uint32_t j = 0; j < n; ++j)
       if ((app < 0 || in[j].app == app) && in[j].n) idx.push_back(j);
     if (idx.empty()) continue;
-    std::stable_sort(idx.begin(), idx.end(),
-                     [&](uint32_t a, uint32_t b) { return walk_cost(in[a]) > walk_cost(in[b]); });
+    if (longest_first)
+      std::stable_sort(idx.begin(), idx.end(),
+                       [&](uint32_t a, uint32_t b) { return walk_cost(in[a]) > walk_cost(in[b]); });
     WalkGroup g{app, table.size(), prefix.size(), (uint32_t)idx.size(), 0};
     uint64_t t = 0;
     prefix.push_back(0);
@@ -754,7 +757,7 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
   cuda_check(cudaGetLastError(), "reserve");
   ++launches_;
-  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
       nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
       base_.as<unsigned long long>(), dev_out_slots);
@@ -832,6 +835,43 @@ void Engine::insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w,
   if (!is_device_ptr(src)) host_check_ids(src, k, n_, "source");
   if (!is_device_ptr(dst)) host_check_ids(dst, k, n_, "destination");
   if (!is_device_ptr(w)) host_check_weights(w, k);
+  const uint64_t c = tuning_.update_chunk;
+  if (c && k > c) {
+    // Sub-batches in batch order append every source's edges in the same
+    // order, so slots and state equal the whole batch's; the whole batch is
+    // checked first, so a bad edge still rejects all of it.
+    check_batch_on_device(src, dst, w, k);
+    for (uint64_t o = 0; o < k; o += c)
+      insert_one(src + o, dst + o, w + o, std::min(c, k - o), out_slots ? out_slots + o : nullptr);
+  } else {
+    insert_one(src, dst, w, k, out_slots);
+  }
+  finish_call();
+}
+
+// Rejects the batch (status, nothing applied) when a device-resident column
+// holds an id >= n or a zero weight; host columns are checked on the host.
+void Engine::check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k) {
+  const uint32_t* da = a && is_device_ptr(a) ? a : nullptr;
+  const uint32_t* db = b && is_device_ptr(b) ? b : nullptr;
+  const uint32_t* dw = w && is_device_ptr(w) ? w : nullptr;
+  if (!da && !db && !dw) return;
+  ctl_.ensure(16, "scratch");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(da, db, dw, k, n_, ctl_.as<uint32_t>(), d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
+  uint32_t ctl = 0;
+  cuda_check(cudaMemcpyAsync(&ctl, ctl_.p, 4, cudaMemcpyDeviceToHost, stream_), "read ctl");
+  cuda_check(cudaStreamSynchronize(stream_), "validate sync");
+  if (ctl) {
+    cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
+    const int st = status_of(ctl);
+    throw Error(st, st == BINGO_ERR_ZERO_WEIGHT ? "batch holds a zero weight" : "batch holds a vertex id >= n");
+  }
+}
+
+void Engine::insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots) {
   ensure_batch_scratch(k);
   const uint32_t* ds = stage(src, k, in_a_, "stage src");
   const uint32_t* dd = stage(dst, k, in_b_, "stage dst");
@@ -846,7 +886,6 @@ void Engine::insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w,
   run_insert(k, dslots, false, k);
   if (out_slots && !dev_out)
     cuda_check(cudaMemcpyAsync(out_slots, dslots, k * 4, cudaMemcpyDeviceToHost, stream_), "slots D2H");
-  finish_call();
 }
 
 void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
@@ -855,6 +894,19 @@ void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   if (!u || !slot) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null delete array");
   if (k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 deletes in one batch");
   if (!is_device_ptr(u)) host_check_ids(u, k, n_, "vertex");
+  const uint64_t c = tuning_.update_chunk;
+  if (c && k > c) {
+    // Sub-batches in batch order run the same swap-remove sequences; skipped
+    // deletes add up in the status word until the one check at the end.
+    check_batch_on_device(u, nullptr, nullptr, k);
+    for (uint64_t o = 0; o < k; o += c) erase_one(u + o, slot + o, std::min(c, k - o));
+  } else {
+    erase_one(u, slot, k);
+  }
+  finish_call();
+}
+
+void Engine::erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   ensure_batch_scratch(k);
   const uint32_t* du = stage(u, k, in_a_, "stage u");
   const uint32_t* dsl = stage(slot, k, in_b_, "stage slot");
@@ -865,12 +917,11 @@ void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   ++launches_;
   group_by_vertex(du, dsl, nullptr, k);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
-  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
       ctl_.as<uint32_t>());
   cuda_check(cudaGetLastError(), "apply delete");
   ++launches_;
-  finish_call();
 }
 
 // Delete by (u, v) pair. No reference counterpart (the reference deletes by
@@ -982,13 +1033,13 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
       throw Error(BINGO_ERR_INVALID_ARGUMENT, "device output must be 32-byte aligned");
   }
   const WalkView W = wview();
-  auto launch = [&](auto kern, unsigned grid, const WalkJobDev& J0, const WalkJobDev* jb, const uint32_t* pf,
+  auto launch = [&](auto kern, unsigned occ, const WalkJobDev& J0, const WalkJobDev* jb, const uint32_t* pf,
                     uint32_t nj, uint32_t tot, uint32_t* qq) {
     cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(grid);
+    lc.gridDim = dim3(grid_for(tot, kBlock, walk_bps(occ, tuning_)));
     lc.blockDim = dim3(kBlock);
     lc.stream = stream_;
-    cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq), "walk launch");
+    cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq, tuning_.walk_chunk), "walk launch");
     ++launches_;
   };
   queue_.ensure(4 * std::max<uint32_t>(n_jobs, 4), "walk queue");
@@ -1001,19 +1052,19 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
       const uint32_t nw = (uint32_t)dj[j].n;
       switch (dj[j].app) {
         case APP_DEEPWALK:
-          launch(k_walk<APP_DEEPWALK, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_DEEPWALK, false>()), dj[j], nullptr,
+          launch(k_walk<APP_DEEPWALK, false>, walk_blocks_per_sm<APP_DEEPWALK, false>(), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
         case APP_NODE2VEC:
-          launch(k_walk<APP_NODE2VEC, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_NODE2VEC, false>()), dj[j], nullptr,
+          launch(k_walk<APP_NODE2VEC, false>, walk_blocks_per_sm<APP_NODE2VEC, false>(), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
         case APP_PPR:
-          launch(k_walk<APP_PPR, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_PPR, false>()), dj[j], nullptr, nullptr, 0,
+          launch(k_walk<APP_PPR, false>, walk_blocks_per_sm<APP_PPR, false>(), dj[j], nullptr, nullptr, 0,
                  nw, q + j);
           break;
         default:
-          launch(k_walk<APP_SAMPLING, false>, grid_for(nw, kBlock, walk_blocks_per_sm<APP_SAMPLING, false>()), dj[j], nullptr,
+          launch(k_walk<APP_SAMPLING, false>, walk_blocks_per_sm<APP_SAMPLING, false>(), dj[j], nullptr,
                  nullptr, 0, nw, q + j);
           break;
       }
@@ -1023,7 +1074,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     std::vector<WalkJobDev> table;
     std::vector<uint32_t> pf;
     std::vector<WalkGroup> groups;
-    build_walk_groups(dj.data(), n_jobs, walk_split_by_app(), table, pf, groups);
+    build_walk_groups(dj.data(), n_jobs, tuning_.walk_split != 0, tuning_.walk_order != 0, table, pf, groups);
     jobs_.ensure(table.size() * sizeof(WalkJobDev), "walk jobs");
     prefix_.ensure(pf.size() * 4, "walk jobs");
     cuda_check(cudaMemcpyAsync(jobs_.p, table.data(), table.size() * sizeof(WalkJobDev), cudaMemcpyHostToDevice,
@@ -1034,7 +1085,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     for (size_t gi = 0; gi < groups.size(); ++gi) {
       const WalkGroup& G = groups[gi];
       launch_walk_table(stream_, G.app, W, table[G.job_off], jobs_.as<WalkJobDev>() + G.job_off,
-                        prefix_.as<uint32_t>() + G.pf_off, G.n_jobs, G.total, q + gi);
+                        prefix_.as<uint32_t>() + G.pf_off, G.n_jobs, G.total, q + gi, tuning_);
       ++launches_;
     }
   }
@@ -1133,7 +1184,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
   cuda_check(cudaGetLastError(), "reserve");
   ++launches_;
-  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
       nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
       base_.as<unsigned long long>(), out_slots);
@@ -1149,7 +1200,7 @@ void Engine::enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k)
   ++launches_;
   group_by_vertex(u, slot, nullptr, k);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
-  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, 8), kBlock, 0, stream_>>>(
+  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
       ctl_.as<uint32_t>());
   cuda_check(cudaGetLastError(), "apply delete");
@@ -1211,7 +1262,9 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
   std::vector<uint32_t> pf;
   std::vector<WalkGroup> groups;
   std::vector<size_t> grp_begin(n_ops, 0), grp_end(n_ops, 0);
-  const bool split = walk_split_by_app();
+  const bool split = tuning_.walk_split != 0;
+  mix(tuning_.walk_chunk), mix(tuning_.walk_blocks_per_sm), mix(tuning_.walk_split), mix(tuning_.walk_order);
+  mix(tuning_.apply_blocks_per_sm);
   dj.reserve(n_jobs_total);
   for (uint32_t i = 0; i < n_ops; ++i) {
     const bingo_op& o = ops[i];
@@ -1254,7 +1307,7 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
       dj.push_back(D);
     }
     grp_begin[i] = groups.size();
-    build_walk_groups(dj.data(), (uint32_t)dj.size(), split, table, pf, groups);
+    build_walk_groups(dj.data(), (uint32_t)dj.size(), split, tuning_.walk_order != 0, table, pf, groups);
     grp_end[i] = groups.size();
   }
   // Job tables are read by the walk kernels from device memory, so their
@@ -1288,7 +1341,7 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
           const WalkGroup& G = groups[gi];
           launch_walk_table(stream_, G.app, W, table[G.job_off], prog_jobs_.as<WalkJobDev>() + G.job_off,
                             prog_prefix_.as<uint32_t>() + G.pf_off, G.n_jobs, G.total,
-                            prog_queue_.as<uint32_t>() + gi);
+                            prog_queue_.as<uint32_t>() + gi, tuning_);
           ++launches_;
         }
       }
@@ -1413,8 +1466,8 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
              "no-alloc prefix H2D");
   cuda_check(cudaMemsetAsync(&scratch->queue, 0, 4, stream_), "no-alloc counter reset");
   const WalkView W = wview();
-  k_walk<-1, true><<<grid_for(total, kBlock, walk_blocks_per_sm<-1, true>()), kBlock, 0, stream_>>>(
-      W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue);
+  k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), tuning_)), kBlock, 0, stream_>>>(
+      W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue, tuning_.walk_chunk);
   cuda_check(cudaGetLastError(), "no-alloc walk launch");
   ++launches_;
   finish_call();
@@ -1567,6 +1620,84 @@ void Engine::dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, ui
       aalias[a] = alt;
     }
   }
+}
+
+// ------------------------------------------------------------------ tuning / state copy
+void StateCopy::release() {
+  vrec.release(), meta.release(), gdesc.release(), gs.release();
+  for (auto& a : arena) a.release();
+}
+
+void Engine::set_tuning(const Tuning& t) {
+  if (t.walk_chunk < 1 || t.walk_chunk > 1024) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_chunk must be in [1, 1024]");
+  if (t.walk_blocks_per_sm > 32) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_blocks_per_sm must be <= 32");
+  if (t.walk_split > 1 || t.walk_order > 1) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_split / walk_order are 0 or 1");
+  if (t.apply_blocks_per_sm < 1 || t.apply_blocks_per_sm > 32)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "apply_blocks_per_sm must be in [1, 32]");
+  tuning_ = t;
+}
+
+// Device copy of the store (used part of each arena); false when the device
+// has no room for it.
+bool Engine::save_state(StateCopy& c) {
+  cuda_check(cudaStreamSynchronize(stream_), "state copy");
+  read_tops();
+  try {
+    c.vrec.ensure((size_t)n_ * sizeof(VertexRec), "state copy");
+    c.meta.ensure((size_t)n_ * sizeof(VertexMeta), "state copy");
+    c.gdesc.ensure((size_t)n_ * kBits * sizeof(GroupDesc), "state copy");
+    for (int a = 0; a < kArenas; ++a) c.arena[a].ensure(std::max(1ull, h_top_[a]) * kUnitBytes[a], "state copy");
+    c.gs.ensure(std::max(1ull, h_top_[A_MEMBER]) * 4, "state copy");
+  } catch (const Error&) {
+    cudaGetLastError();
+    c.release();
+    return false;
+  }
+  cuda_check(cudaMemcpyAsync(c.vrec.p, vrec_.p, (size_t)n_ * sizeof(VertexRec), cudaMemcpyDeviceToDevice, stream_),
+             "state copy");
+  cuda_check(cudaMemcpyAsync(c.meta.p, meta_.p, (size_t)n_ * sizeof(VertexMeta), cudaMemcpyDeviceToDevice, stream_),
+             "state copy");
+  cuda_check(cudaMemcpyAsync(c.gdesc.p, gdesc_.p, (size_t)n_ * kBits * sizeof(GroupDesc), cudaMemcpyDeviceToDevice,
+                             stream_),
+             "state copy");
+  for (int a = 0; a < kArenas; ++a) {
+    c.top[a] = h_top_[a];
+    if (h_top_[a])
+      cuda_check(cudaMemcpyAsync(c.arena[a].p, arena_[a].p, h_top_[a] * kUnitBytes[a], cudaMemcpyDeviceToDevice,
+                                 stream_),
+                 "state copy");
+  }
+  if (h_top_[A_MEMBER])
+    cuda_check(cudaMemcpyAsync(c.gs.p, gs_.p, h_top_[A_MEMBER] * 4, cudaMemcpyDeviceToDevice, stream_), "state copy");
+  cuda_check(cudaStreamSynchronize(stream_), "state copy");
+  return true;
+}
+
+// Puts a copy back. Arenas only grow, so each still holds the copy's used
+// part at the same offsets.
+void Engine::restore_state(const StateCopy& c) {
+  cuda_check(cudaStreamSynchronize(stream_), "state restore");
+  cuda_check(cudaMemcpyAsync(vrec_.p, c.vrec.p, (size_t)n_ * sizeof(VertexRec), cudaMemcpyDeviceToDevice, stream_),
+             "state restore");
+  cuda_check(cudaMemcpyAsync(meta_.p, c.meta.p, (size_t)n_ * sizeof(VertexMeta), cudaMemcpyDeviceToDevice, stream_),
+             "state restore");
+  cuda_check(cudaMemcpyAsync(gdesc_.p, c.gdesc.p, (size_t)n_ * kBits * sizeof(GroupDesc), cudaMemcpyDeviceToDevice,
+                             stream_),
+             "state restore");
+  for (int a = 0; a < kArenas; ++a) {
+    if (c.top[a] > cap_[a]) throw Error(BINGO_ERR_CUDA, "state copy larger than its arena");
+    if (c.top[a])
+      cuda_check(cudaMemcpyAsync(arena_[a].p, c.arena[a].p, c.top[a] * kUnitBytes[a], cudaMemcpyDeviceToDevice,
+                                 stream_),
+                 "state restore");
+    h_top_[a] = c.top[a];
+  }
+  if (c.top[A_MEMBER])
+    cuda_check(cudaMemcpyAsync(gs_.p, c.gs.p, c.top[A_MEMBER] * 4, cudaMemcpyDeviceToDevice, stream_), "state restore");
+  cuda_check(cudaMemcpyAsync(d_top_, h_top_, kArenas * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_),
+             "state restore");
+  cuda_check(cudaMemsetAsync(d_err_, 0, 2 * sizeof(uint32_t), stream_), "state restore");
+  cuda_check(cudaStreamSynchronize(stream_), "state restore");
 }
 
 }  // namespace bingo

@@ -37,6 +37,25 @@ struct DevBuf {
 
 class Server;
 
+// Launch and batching knobs (bingo_tuning); none changes any result.
+struct Tuning {
+  uint32_t walk_chunk = 32;
+  uint32_t walk_blocks_per_sm = 0;  // 0 = occupancy limit
+  uint32_t walk_split = 0;
+  uint32_t walk_order = 1;
+  uint32_t update_chunk = 0;  // 0 = whole batch
+  uint32_t apply_blocks_per_sm = 8;
+};
+
+// A device copy of the graph store (the update knobs are timed on the live
+// graph and undone from it).
+struct StateCopy {
+  DevBuf vrec, meta, gdesc, gs;
+  DevBuf arena[kArenas];
+  unsigned long long top[kArenas] = {};
+  void release();
+};
+
 class Engine {
  public:
   explicit Engine(const bingo_config& cfg);
@@ -59,6 +78,9 @@ class Engine {
             uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT, uint8_t* aown,
             uint8_t* aalias);
   void philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
+  const Tuning& tuning() const { return tuning_; }
+  void set_tuning(const Tuning& t);
+  void autotune(const bingo_tune_request& req, bingo_tune_report* out);
 
   std::string last_error;
   cudaStream_t stream() const { return stream_; }
@@ -109,6 +131,7 @@ class Engine {
   uint64_t graph_sig_ = 0, graph_launches_ = 0;
   uint64_t arena_gen_ = 0;  // bumped whenever an arena or the vertex arrays are reallocated
   std::unique_ptr<Server> server_;
+  Tuning tuning_;
 
   StoreView view() const;
   WalkView wview() const;
@@ -125,6 +148,11 @@ class Engine {
   void read_tops();
   void finish_call();
   void require_loaded() const;
+  void insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
+  void erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k);
+  void check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k);
+  bool save_state(StateCopy& c);
+  void restore_state(const StateCopy& c);
 };
 
 bool is_device_ptr(const void* p);

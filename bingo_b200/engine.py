@@ -14,8 +14,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import (BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeMetrics, BingoServeStatus,
-                   BingoStats, BingoWalkJob, lib)
+from ._lib import (TUNING_FIELDS, BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeMetrics,
+                   BingoServeStatus, BingoStats, BingoTuneReport, BingoTuneRequest, BingoTuning, BingoWalkJob, lib)
 
 DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
@@ -277,6 +277,51 @@ class Graph:
         self._check(self._L.bingo_serve_wait(self._h, ticket, timeout_us, ctypes.byref(s)))
         self._serve_keep.pop(ticket, None)
         return self._status(s)
+
+    # ------------------------------------------------------------ tuning
+    def tuning(self) -> dict:
+        """Current launch / batching knobs (bingo_get_tuning)."""
+        t = BingoTuning()
+        self._check(self._L.bingo_get_tuning(self._h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f in TUNING_FIELDS}
+
+    def set_tuning(self, **knobs):
+        """Change some knobs, keeping the others (bingo_set_tuning)."""
+        cur = self.tuning()
+        unknown = set(knobs) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning knobs {sorted(unknown)}")
+        cur.update(knobs)
+        t = BingoTuning(*[cur[f] for f in TUNING_FIELDS])
+        self._check(self._L.bingo_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, jobs: Sequence[WalkJob] = (), inserts=None, deletes=None, repeats: int = 3) -> dict:
+        """Time the sample workload under candidate knobs and keep the fastest
+        (bingo_autotune). inserts = (src, dst, w), deletes = (u, slot); the
+        update sample is undone, so the graph is unchanged."""
+        keep = []
+        req = BingoTuneRequest()
+        if jobs:
+            arr = self._job_array(list(jobs), keep)
+            keep.append(arr)
+            req.jobs = ctypes.cast(arr, ctypes.c_void_p)
+            req.n_jobs = len(jobs)
+        req.repeats = repeats
+        if inserts is not None:
+            cols = [_u32(x) for x in inserts]
+            keep += [c[1] for c in cols]
+            req.ins_src, req.ins_dst, req.ins_w = (c[0] for c in cols)
+            req.n_ins = len(inserts[0]) if not hasattr(inserts[0], "numel") else inserts[0].numel()
+        if deletes is not None:
+            cols = [_u32(x) for x in deletes]
+            keep += [c[1] for c in cols]
+            req.del_u, req.del_slot = (c[0] for c in cols)
+            req.n_del = len(deletes[0]) if not hasattr(deletes[0], "numel") else deletes[0].numel()
+        rep = BingoTuneReport()
+        self._check(self._L.bingo_autotune(self._h, ctypes.byref(req), ctypes.byref(rep)))
+        out = {f: getattr(rep, f) for f, _ in BingoTuneReport._fields_ if f not in ("best", "reserved0")}
+        out["best"] = {f: getattr(rep.best, f) for f in TUNING_FIELDS}
+        return out
 
     def serve_metrics(self) -> dict:
         m = BingoServeMetrics()

@@ -233,6 +233,54 @@ int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, 
 int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);
 /* Waits at most timeout_us; returns BINGO_ERR_TIMEOUT if the ticket is not done. */
 int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out);
+/* ---- Tuning -------------------------------------------------------------
+ * Launch and batching parameters. None of them changes any result (walks,
+ * slot ids, graph state); bingo_autotune picks them by measurement. */
+typedef struct bingo_tuning {
+  uint32_t walk_chunk;          /* walks a warp claims per refill, 1..1024 (default 32) */
+  uint32_t walk_blocks_per_sm;  /* resident walk blocks per SM, 0 = the occupancy limit (default) */
+  uint32_t walk_split;          /* 1: one persistent launch per app; 0: one mixed launch (default) */
+  uint32_t walk_order;          /* 1: jobs with the longest expected walks first (default); 0: job order */
+  uint32_t update_chunk;        /* edges per update sub-batch of bingo_insert_batch / bingo_delete_batch,
+                                   0 = the whole batch (default) */
+  uint32_t apply_blocks_per_sm; /* blocks per SM of the insert / delete apply kernels, 1..32 (default 8) */
+  uint32_t reserved[2];
+} bingo_tuning;
+
+int bingo_get_tuning(bingo_handle* h, bingo_tuning* out);
+int bingo_set_tuning(bingo_handle* h, const bingo_tuning* t);
+
+/* Sample workload for bingo_autotune. The walk jobs follow bingo_walk
+ * (BINGO_WALK_BATCHED; their outputs are overwritten). The optional update
+ * batch (inserts, then deletes by slot valid against the current graph) is
+ * timed on the handle's graph and undone from a device copy taken first, so
+ * the graph is unchanged when the call returns; without room for the copy
+ * the update knobs are left as they are. */
+typedef struct bingo_tune_request {
+  const bingo_walk_job* jobs;
+  uint32_t n_jobs;
+  uint32_t repeats;  /* timed runs per candidate (0 = 3); the median counts */
+  const uint32_t *ins_src, *ins_dst, *ins_w;
+  uint64_t n_ins;
+  const uint32_t *del_u, *del_slot;
+  uint64_t n_del;
+} bingo_tune_request;
+
+typedef struct bingo_tune_report {
+  bingo_tuning best;         /* also made current */
+  double walk_ms_start;      /* median wall time of the job set with the starting knobs */
+  double walk_ms_best;
+  double update_ms_start;    /* median wall time of the update batch (-1: not tuned) */
+  double update_ms_best;
+  uint32_t candidates;       /* configurations timed */
+  uint32_t reserved0;
+} bingo_tune_report;
+
+/* Coordinate search: walk_chunk, walk_split, walk_order, walk_blocks_per_sm,
+ * then update_chunk and apply_blocks_per_sm; a candidate replaces the
+ * current choice when its median is at least 1 % lower. */
+int bingo_autotune(bingo_handle* h, const bingo_tune_request* req, bingo_tune_report* out);
+
 /* Scheduler counters since bingo_serve_start (times in ns of scheduler-thread wall time). */
 typedef struct bingo_serve_metrics {
   uint64_t submitted, completed;
