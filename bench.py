@@ -437,6 +437,7 @@ def run_served(args):
     for t in wt:
         g.serve_wait(t, timeout_us=600_000_000)
     g.serve_stop()
+    prepare(0)
     for (k, _, x), o in zip(wu, wouts):
         if k == "walk":
             g.walk(app=x[0], length=WALK_LEN, starts=x[1], seed=7, job_id=x[2], stop_prob=0.15, out=o)

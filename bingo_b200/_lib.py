@@ -157,6 +157,9 @@ SIGNATURES = {
                                         c_void_p, c_void_p]),
     "bingo_updgen_deletes": (c_uint64, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "bingo_updgen_live": (c_uint64, [c_void_p]),
+    "bingo_edge_list_read": (c_int, [ctypes.c_char_p, c_void_p, c_void_p, c_uint64, POINTER(c_uint64),
+                                     POINTER(c_uint32)]),
+    "bingo_driver_weights": (c_int, [c_int, c_void_p, c_void_p, c_uint64, c_uint32, c_void_p]),
 }
 
 _lib = None

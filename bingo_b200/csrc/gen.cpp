@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -219,6 +220,88 @@ uint64_t bingo_updgen_deletes(bingo_updgen* g, uint64_t k, uint32_t* u, uint32_t
     u[made] = e.u, slot[made] = e.slot;
   }
   return made;
+}
+
+// ---- the reference's own inputs (include/graph.cuh:22-51) -------------------
+
+int bingo_edge_list_read(const char* path, uint32_t* src, uint32_t* dst, uint64_t cap, uint64_t* m, uint32_t* n) {
+  if (!path || !m || !n) return -1;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return -1;
+  std::vector<char> buf(1 << 22);
+  uint64_t count = 0, offset = 0, maxid = 0;
+  uint64_t val = 0, pair[2] = {0, 0};
+  int state = 0;       // 0 between tokens, 1 in a number, 2 in a comment line
+  int half = 0;        // ids of the current pair read so far
+  bool line_start = true;
+  int rc = 0;
+  auto emit = [&](uint64_t x) -> int {
+    if (x > 0xFFFFFFFEull) return -4;
+    pair[half++] = x;
+    if (half == 2) {
+      if (src) {
+        if (count >= cap) return -3;
+        src[count] = (uint32_t)pair[0], dst[count] = (uint32_t)pair[1];
+      }
+      maxid = std::max(maxid, std::max(pair[0], pair[1]));
+      ++count;
+      half = 0;
+    }
+    return 0;
+  };
+  size_t got;
+  while (rc == 0 && (got = std::fread(buf.data(), 1, buf.size(), f)) > 0) {
+    for (size_t i = 0; i < got && rc == 0; ++i, ++offset) {
+      const char c = buf[i];
+      if (state == 2) {
+        if (c == '\n') state = 0, line_start = true;
+        continue;
+      }
+      if (c >= '0' && c <= '9') {
+        if (state == 0) val = 0, state = 1;
+        val = val * 10 + (uint64_t)(c - '0');
+        if (val > 0xFFFFFFFFull) val = 0x100000000ull;  // saturate; rejected as too large
+        line_start = false;
+      } else if (c == ' ' || c == '\t' || c == '\r' || c == '\n') {
+        if (state == 1) rc = emit(val), state = 0;
+        if (c == '\n') line_start = true;
+      } else if ((c == '#' || c == '%') && line_start && state == 0) {
+        state = 2;
+      } else {
+        *m = offset;
+        rc = -2;
+      }
+    }
+  }
+  if (std::ferror(f) && rc == 0) rc = -1;
+  std::fclose(f);
+  if (rc == 0 && state == 1) rc = emit(val);
+  if (rc == 0 && half) {  // a trailing lone id: the reference's scanf("%d%d") would not form an edge
+    *m = offset;
+    rc = -2;
+  }
+  if (rc) return rc;
+  *m = count;
+  *n = count ? (uint32_t)(maxid + 1) : 0;
+  return 0;
+}
+
+int bingo_driver_weights(int kind, const uint32_t* src, const uint32_t* dst, uint64_t m, uint32_t n, uint32_t* w) {
+  if (kind == BINGO_DRIVER_AUTO) kind = n > 1e7 ? BINGO_DRIVER_DEGREE_POW03 : BINGO_DRIVER_DEGREE;
+  if (kind != BINGO_DRIVER_DEGREE && kind != BINGO_DRIVER_DEGREE_POW03) return -1;
+  std::vector<uint32_t> d(n, 0);
+  for (uint64_t i = 0; i < m; ++i) {
+    if (src[i] >= n || dst[i] >= n) return -1;
+    ++d[src[i]];
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; ++i) {
+    const uint32_t dv = d[dst[i]];
+    // The reference computes int w = bias(d) + 1 with bias returning float.
+    const float b = kind == BINGO_DRIVER_DEGREE ? (float)dv : (float)std::pow((double)dv, 0.3);
+    w[i] = (uint32_t)(b + 1.0f);
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -5,12 +5,15 @@ files (include/graph.cuh:22-27) and its update generators
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
 from ._lib import lib
 
 W_UNIFORM, W_LOGUNIFORM, W_ZIPF = 0, 1, 2
+DRIVER_AUTO, DRIVER_DEGREE, DRIVER_DEGREE_POW03 = 0, 1, 2
+_READ_ERRORS = {-1: "cannot open or read", -2: "malformed token", -3: "arrays too small", -4: "id above 2^32 - 2"}
 
 
 def _p(a):
@@ -63,3 +66,32 @@ class UpdateGen:
         if getattr(self, "_g", None):
             self._L.bingo_updgen_destroy(self._g)
             self._g = None
+
+
+def read_edge_list(path: str):
+    """An edge-list file as the reference's loadGraph() reads it ("u v" pairs,
+    include/graph.cuh:22-27; '#'/'%' comment lines skipped). Returns
+    (src, dst, n) with ids as in the file and n = largest id + 1."""
+    L = lib()
+    m, n = ctypes.c_uint64(), ctypes.c_uint32()
+    bp = os.fsencode(path)
+    rc = L.bingo_edge_list_read(bp, None, None, 0, ctypes.byref(m), ctypes.byref(n))
+    if rc:
+        raise ValueError(f"{path}: {_READ_ERRORS.get(rc, rc)}" + (f" at byte {m.value}" if rc == -2 else ""))
+    src = np.empty(m.value, np.uint32)
+    dst = np.empty(m.value, np.uint32)
+    rc = L.bingo_edge_list_read(bp, _p(src), _p(dst), len(src), ctypes.byref(m), ctypes.byref(n))
+    if rc:
+        raise ValueError(f"{path}: {_READ_ERRORS.get(rc, rc)}")
+    return src, dst, int(n.value)
+
+
+def driver_weights(src, dst, n: int, kind: int = DRIVER_AUTO):
+    """The reference driver's load weights: trunc(bias(outdeg(v))) + 1 with
+    bias(d) = d, or d^0.3 for n > 1e7 (include/graph.cuh:43-51, include/api.h:29-30)."""
+    s, d = np.ascontiguousarray(src, np.uint32), np.ascontiguousarray(dst, np.uint32)
+    w = np.empty(len(s), np.uint32)
+    if lib().bingo_driver_weights(kind, _p(s), _p(d), len(s), n, _p(w)):
+        raise ValueError("unknown weight kind or an id >= n")
+    return w
+

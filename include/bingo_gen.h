@@ -50,6 +50,32 @@ uint64_t bingo_updgen_inserts(bingo_updgen* g, uint64_t k, int dist, double lo, 
 uint64_t bingo_updgen_deletes(bingo_updgen* g, uint64_t k, uint32_t* u, uint32_t* slot);
 uint64_t bingo_updgen_live(const bingo_updgen* g);
 
+/* ---- The reference's own inputs ------------------------------------------
+ * Edge-list files as the reference's loadGraph() reads them
+ * (include/graph.cuh:22-27): whitespace-separated "u v" pairs of
+ * non-negative decimal ids, one edge per pair, kept in file order (self-loops
+ * and duplicates too, as the reference keeps them). Unlike the reference's
+ * scanf loop, lines starting with '#' or '%' (SNAP / Matrix Market headers)
+ * are skipped. Ids stay as in the file (the engine is 0-based; the reference
+ * adds 1 and keeps vertex 0 as scratch), and n = largest id + 1.
+ *
+ * Two calls: bingo_edge_list_read(path, NULL, NULL, 0, &m, &n) counts;
+ * a second call with arrays of at least m entries fills them. Returns 0, or
+ * -1 (cannot open / read), -2 (malformed token at byte offset *m), -3
+ * (arrays too small), -4 (an id above 2^32 - 2). */
+int bingo_edge_list_read(const char* path, uint32_t* src, uint32_t* dst, uint64_t cap, uint64_t* m, uint32_t* n);
+
+/* Load weights of the reference driver (include/graph.cuh:43-51,
+ * include/api.h:29-30): w = trunc(bias(d(v))) + 1 with d(v) the out-degree
+ * of the edge's destination over the edge list, bias(d) = d
+ * (BINGO_DRIVER_DEGREE) or (float)pow(d, 0.3) (BINGO_DRIVER_DEGREE_POW03);
+ * BINGO_DRIVER_AUTO picks the second when n > 1e7, as the reference does.
+ * Returns 0, or -1 for an unknown kind or an id >= n. */
+#define BINGO_DRIVER_AUTO 0
+#define BINGO_DRIVER_DEGREE 1
+#define BINGO_DRIVER_DEGREE_POW03 2
+int bingo_driver_weights(int kind, const uint32_t* src, const uint32_t* dst, uint64_t m, uint32_t n, uint32_t* w);
+
 #ifdef __cplusplus
 }
 #endif
