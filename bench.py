@@ -14,6 +14,7 @@ rank runs a full replica (weak scaling, no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import re
@@ -453,6 +454,8 @@ def run_served(args):
         prepare(ri)
         s0 = g.stats()["walk_steps"]
         g.serve_start(output_budget_bytes=args.serve_budget << 20, max_update_batch=1 << 20, idle_timeout_us=3000)
+        gc.collect()
+        gc.disable()  # no collector pauses inside either arm's timed region
         t0 = time.monotonic_ns()
         tickets = []
         for (kind, at, x), out in zip(tr, outs):
@@ -472,6 +475,7 @@ def run_served(args):
             assert st["status"] == 0, st
             lat["walk" if kind == "walk" else "update"].append((st["ready_ns"] - due) / 1e6)
             last_ready = max(last_ready, st["ready_ns"])
+        gc.enable()
         smet = g.serve_metrics()
         g.serve_stop()
         served_steps = g.stats()["walk_steps"] - s0
@@ -480,11 +484,15 @@ def run_served(args):
         prepare(ri)
         s0 = g.stats()["walk_steps"]
         plat = {"walk": [], "update": []}
+        ptrace = []
+        gc.collect()
+        gc.disable()
         t0 = time.monotonic_ns()
         for (kind, at, x), out in zip(tr, outs):
             due = t0 + int(at * 1e9)
             while time.monotonic_ns() < due:
                 pass
+            t_call = time.monotonic_ns()
             if kind == "walk":
                 app, starts, jid = x
                 g.walk(app=app, length=WALK_LEN, starts=starts, seed=7, job_id=jid, stop_prob=0.15, out=out)
@@ -493,7 +501,10 @@ def run_served(args):
             else:
                 g.delete_batch(*x)
             plat["walk" if kind == "walk" else "update"].append((time.monotonic_ns() - due) / 1e6)
+            ptrace.append((kind, len(x[1]) if kind == "walk" else len(x[0]), round((time.monotonic_ns() - due) / 1e6, 3),
+                           round((time.monotonic_ns() - t_call) / 1e6, 3)))
         plain_span = (time.monotonic_ns() - t0) / 1e9
+        gc.enable()
         plain_steps = g.stats()["walk_steps"] - s0
         n_walk = len(lat["walk"])
         upd_edges = sum(len(x[0]) for kind, _, x in tr if kind != "walk")
@@ -507,7 +518,7 @@ def run_served(args):
             "plain": {"walk_p50_ms": pct(plat["walk"], 50), "walk_p99_ms": pct(plat["walk"], 99),
                       "update_p50_ms": pct(plat["update"], 50), "update_p99_ms": pct(plat["update"], 99),
                       "walk_steps_per_s": plain_steps / plain_span, "requests_per_s": len(tr) / plain_span,
-                      "span_s": plain_span},
+                      "span_s": plain_span, "slowest_requests": sorted(((i,) + t for i, t in enumerate(ptrace)), key=lambda z: -z[4])[:8]},
         })
     best = max(results, key=lambda r: r["served"]["walk_steps_per_s"])
     line = {"metric": "walk_steps_per_s", "value": best["served"]["walk_steps_per_s"], "unit": "steps/s",

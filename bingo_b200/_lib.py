@@ -140,6 +140,8 @@ SIGNATURES = {
     "bingo_serve_wait": (c_int, [c_void_p, c_uint64, c_uint64, POINTER(BingoServeStatus)]),
     "bingo_serve_stop": (c_int, [c_void_p]),
     "bingo_serve_get_metrics": (c_int, [c_void_p, POINTER(BingoServeMetrics)]),
+    "bingo_save": (c_int, [c_void_p, ctypes.c_char_p]),
+    "bingo_restore": (c_int, [c_void_p, ctypes.c_char_p]),
     "bingo_get_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
     "bingo_set_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
     "bingo_autotune": (c_int, [c_void_p, POINTER(BingoTuneRequest), POINTER(BingoTuneReport)]),

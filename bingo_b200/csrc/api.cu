@@ -146,6 +146,14 @@ int bingo_get_stats(bingo_handle* h, bingo_stats* out) {
   return guarded(h, [&](bingo::Engine& e) { e.stats(out); }, true);
 }
 
+int bingo_save(bingo_handle* h, const char* path) {
+  return guarded(h, [&](bingo::Engine& e) { e.save(path); });
+}
+
+int bingo_restore(bingo_handle* h, const char* path) {
+  return guarded(h, [&](bingo::Engine& e) { e.restore(path); });
+}
+
 int bingo_get_tuning(bingo_handle* h, bingo_tuning* out) {
   if (!out) return BINGO_ERR_INVALID_ARGUMENT;
   return guarded(

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -1698,6 +1699,215 @@ void Engine::restore_state(const StateCopy& c) {
              "state restore");
   cuda_check(cudaMemsetAsync(d_err_, 0, 2 * sizeof(uint32_t), stream_), "state restore");
   cuda_check(cudaStreamSynchronize(stream_), "state restore");
+}
+
+// ------------------------------------------------------------------ snapshot files
+// Layout: SnapHeader, then the vertex arrays (VertexRec, VertexMeta,
+// GroupDesc x 32 per vertex), each arena's used part in arena order and the
+// member slot ids, all as the device holds them (offsets stay valid because
+// the arenas are restored at the same positions). The checksum covers the
+// payload; record sizes and the format version guard against a file from an
+// incompatible build.
+namespace {
+
+struct SnapHeader {
+  char magic[8];
+  uint32_t version, node2vec, n, bits;
+  uint32_t rec_bytes[4];  // VertexRec, VertexMeta, GroupDesc, AliasRec
+  uint64_t top[kArenas];
+  uint64_t payload_bytes;
+  uint64_t checksum;
+};
+constexpr char kSnapMagic[8] = {'B', 'I', 'N', 'G', 'O', 'S', 'N', 'P'};
+constexpr uint32_t kSnapVersion = 1;
+constexpr size_t kSnapChunk = 64u << 20;
+
+// Word-wise multiply-xor hash (64-bit lanes, tail bytes folded in one by one).
+struct SnapSum {
+  uint64_t h = 0x9E3779B97F4A7C15ull;
+  void add(const char* p, size_t b) {
+    size_t i = 0;
+    for (; i + 8 <= b; i += 8) {
+      uint64_t x;
+      std::memcpy(&x, p + i, 8);
+      h = (h ^ x) * 0x100000001B3ull;
+      h ^= h >> 29;
+    }
+    for (; i < b; ++i) h = (h ^ (uint8_t)p[i]) * 0x100000001B3ull;
+  }
+};
+
+struct Pinned {
+  char* p = nullptr;
+  explicit Pinned(size_t b) { cuda_check(cudaMallocHost((void**)&p, b), "snapshot staging"); }
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+struct File {
+  FILE* f = nullptr;
+  File(const char* path, const char* mode) : f(std::fopen(path, mode)) {}
+  ~File() {
+    if (f) std::fclose(f);
+  }
+};
+
+}  // namespace
+
+void Engine::save(const char* path) {
+  require_loaded();
+  require_idle();
+  if (!path) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null path");
+  cuda_check(cudaStreamSynchronize(stream_), "snapshot");
+  read_tops();
+  struct Part {
+    const void* dev;
+    uint64_t bytes;
+  };
+  std::vector<Part> parts = {{vrec_.p, (uint64_t)n_ * sizeof(VertexRec)},
+                             {meta_.p, (uint64_t)n_ * sizeof(VertexMeta)},
+                             {gdesc_.p, (uint64_t)n_ * kBits * sizeof(GroupDesc)}};
+  for (int a = 0; a < kArenas; ++a) parts.push_back({arena_[a].p, h_top_[a] * kUnitBytes[a]});
+  parts.push_back({gs_.p, h_top_[A_MEMBER] * 4});
+  SnapHeader H{};
+  std::memcpy(H.magic, kSnapMagic, 8);
+  H.version = kSnapVersion;
+  H.node2vec = cfg_.node2vec ? 1 : 0;
+  H.n = n_;
+  H.bits = kBits;
+  H.rec_bytes[0] = sizeof(VertexRec), H.rec_bytes[1] = sizeof(VertexMeta);
+  H.rec_bytes[2] = sizeof(GroupDesc), H.rec_bytes[3] = sizeof(AliasRec);
+  for (int a = 0; a < kArenas; ++a) H.top[a] = h_top_[a];
+  for (const Part& q : parts) H.payload_bytes += q.bytes;
+  File F(path, "wb");
+  if (!F.f) throw Error(BINGO_ERR_INVALID_ARGUMENT, std::string("cannot create ") + path);
+  if (std::fwrite(&H, sizeof H, 1, F.f) != 1) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot write failed");
+  // Double-buffered: the copy of the next chunk overlaps the write of this one.
+  Pinned stage(2 * kSnapChunk);
+  cudaEvent_t ev[2];
+  cuda_check(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "event");
+  cuda_check(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "event");
+  SnapSum sum;
+  struct Pending {
+    size_t bytes = 0;
+    int buf = 0;
+  } pend;
+  bool have = false;
+  int next = 0;
+  auto drain = [&]() {
+    cuda_check(cudaEventSynchronize(ev[pend.buf]), "snapshot copy");
+    const char* p = stage.p + (size_t)pend.buf * kSnapChunk;
+    sum.add(p, pend.bytes);
+    if (std::fwrite(p, 1, pend.bytes, F.f) != pend.bytes) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot write failed");
+    have = false;
+  };
+  try {
+    for (const Part& q : parts)
+      for (uint64_t o = 0; o < q.bytes; o += kSnapChunk) {
+        const size_t b = (size_t)std::min<uint64_t>(kSnapChunk, q.bytes - o);
+        cuda_check(cudaMemcpyAsync(stage.p + (size_t)next * kSnapChunk, (const char*)q.dev + o, b,
+                                   cudaMemcpyDeviceToHost, stream_),
+                   "snapshot copy");
+        cuda_check(cudaEventRecord(ev[next], stream_), "event");
+        if (have) drain();
+        pend = Pending{b, next};
+        have = true;
+        next ^= 1;
+      }
+    if (have) drain();
+  } catch (...) {
+    cudaStreamSynchronize(stream_);
+    cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+    throw;
+  }
+  cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+  H.checksum = sum.h;
+  if (std::fseek(F.f, 0, SEEK_SET) || std::fwrite(&H, sizeof H, 1, F.f) != 1 || std::fflush(F.f))
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot write failed");
+}
+
+void Engine::restore(const char* path) {
+  require_idle();
+  if (!path) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null path");
+  File F(path, "rb");
+  if (!F.f) throw Error(BINGO_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+  SnapHeader H{};
+  if (std::fread(&H, sizeof H, 1, F.f) != 1 || std::memcmp(H.magic, kSnapMagic, 8))
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "not a graph snapshot");
+  if (H.version != kSnapVersion || H.bits != (uint32_t)kBits || H.rec_bytes[0] != sizeof(VertexRec) ||
+      H.rec_bytes[1] != sizeof(VertexMeta) || H.rec_bytes[2] != sizeof(GroupDesc) || H.rec_bytes[3] != sizeof(AliasRec))
+    throw Error(BINGO_ERR_UNSUPPORTED, "snapshot from an incompatible build");
+  if (H.node2vec != (cfg_.node2vec ? 1u : 0u))
+    throw Error(BINGO_ERR_UNSUPPORTED, H.node2vec ? "snapshot carries the node2vec adjacency index; create the handle "
+                                                    "with config.node2vec = 1"
+                                                  : "snapshot has no node2vec adjacency index; create the handle with "
+                                                    "config.node2vec = 0");
+  if (!H.n) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot with n = 0");
+  uint64_t expect = (uint64_t)H.n * (sizeof(VertexRec) + sizeof(VertexMeta) + kBits * sizeof(GroupDesc));
+  for (int a = 0; a < kArenas; ++a) {
+    if (H.top[a] > kArenaLimit[a]) throw Error(BINGO_ERR_INVALID_ARGUMENT, "corrupt snapshot header");
+    expect += H.top[a] * kUnitBytes[a];
+  }
+  expect += H.top[A_MEMBER] * 4;
+  if (expect != H.payload_bytes) throw Error(BINGO_ERR_INVALID_ARGUMENT, "corrupt snapshot header");
+  cuda_check(cudaStreamSynchronize(stream_), "restore");
+  // From here the handle's old graph is gone; on failure it holds none.
+  loaded_ = false;
+  drop_graph();
+  ++arena_gen_;
+  n_ = H.n;
+  vrec_.release(), meta_.release(), gdesc_.release();
+  vrec_.ensure((size_t)n_ * sizeof(VertexRec), "vertex records");
+  meta_.ensure((size_t)n_ * sizeof(VertexMeta), "vertex metadata");
+  gdesc_.ensure((size_t)n_ * kBits * sizeof(GroupDesc), "group descriptors");
+  const unsigned long long need[kArenas] = {H.top[0], H.top[1], H.top[2], H.top[3], H.top[4]};
+  alloc_arenas(need);
+  struct Part {
+    void* dev;
+    uint64_t bytes;
+  };
+  std::vector<Part> parts = {{vrec_.p, (uint64_t)n_ * sizeof(VertexRec)},
+                             {meta_.p, (uint64_t)n_ * sizeof(VertexMeta)},
+                             {gdesc_.p, (uint64_t)n_ * kBits * sizeof(GroupDesc)}};
+  for (int a = 0; a < kArenas; ++a) parts.push_back({arena_[a].p, H.top[a] * kUnitBytes[a]});
+  parts.push_back({gs_.p, H.top[A_MEMBER] * 4});
+  // Double-buffered: reading the next chunk overlaps the copy of this one;
+  // a half is refilled only after the copy issued from it has finished.
+  Pinned stage(2 * kSnapChunk);
+  cudaEvent_t ev[2];
+  cuda_check(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "event");
+  cuda_check(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "event");
+  bool used[2] = {false, false};
+  SnapSum sum;
+  int next = 0;
+  try {
+    for (const Part& q : parts)
+      for (uint64_t o = 0; o < q.bytes; o += kSnapChunk) {
+        const size_t b = (size_t)std::min<uint64_t>(kSnapChunk, q.bytes - o);
+        char* p = stage.p + (size_t)next * kSnapChunk;
+        if (used[next]) cuda_check(cudaEventSynchronize(ev[next]), "restore copy");
+        if (std::fread(p, 1, b, F.f) != b) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot file is truncated");
+        sum.add(p, b);
+        cuda_check(cudaMemcpyAsync((char*)q.dev + o, p, b, cudaMemcpyHostToDevice, stream_), "restore copy");
+        cuda_check(cudaEventRecord(ev[next], stream_), "event");
+        used[next] = true;
+        next ^= 1;
+      }
+    cuda_check(cudaStreamSynchronize(stream_), "restore copy");
+  } catch (...) {
+    cudaStreamSynchronize(stream_);
+    cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+    throw;
+  }
+  cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+  if (sum.h != H.checksum) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot checksum mismatch");
+  for (int a = 0; a < kArenas; ++a) h_top_[a] = H.top[a];
+  cuda_check(cudaMemcpyAsync(d_top_, h_top_, kArenas * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_),
+             "restore");
+  cuda_check(cudaMemsetAsync(d_err_, 0, 2 * sizeof(uint32_t), stream_), "restore");
+  cuda_check(cudaStreamSynchronize(stream_), "restore");
+  loaded_ = true;
 }
 
 }  // namespace bingo

@@ -78,6 +78,8 @@ class Engine {
             uint32_t* mv, uint32_t* mbp, uint32_t* am, uint64_t* athr, uint64_t* aT, uint8_t* aown,
             uint8_t* aalias);
   void philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
+  void save(const char* path);
+  void restore(const char* path);
   const Tuning& tuning() const { return tuning_; }
   void set_tuning(const Tuning& t);
   void autotune(const bingo_tune_request& req, bingo_tune_report* out);

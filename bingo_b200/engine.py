@@ -9,6 +9,7 @@ ids are 0-based. Errors raise `BingoError` carrying the C status.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 from typing import Optional, Sequence
 
@@ -277,6 +278,16 @@ class Graph:
         self._check(self._L.bingo_serve_wait(self._h, ticket, timeout_us, ctypes.byref(s)))
         self._serve_keep.pop(ticket, None)
         return self._status(s)
+
+    # ------------------------------------------------------------ snapshots
+    def save(self, path):
+        """Write the whole graph store to a file (bingo_save)."""
+        self._check(self._L.bingo_save(self._h, os.fsencode(path)))
+
+    def restore(self, path):
+        """Replace this handle's graph with a saved one (bingo_restore)."""
+        self._check(self._L.bingo_restore(self._h, os.fsencode(path)))
+        self.n = self.stats()["n"]
 
     # ------------------------------------------------------------ tuning
     def tuning(self) -> dict:

@@ -233,6 +233,17 @@ int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, 
 int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);
 /* Waits at most timeout_us; returns BINGO_ERR_TIMEOUT if the ticket is not done. */
 int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bingo_serve_status* out);
+/* ---- Snapshots ------------------------------------------------------------
+ * No reference counterpart (the reference rebuilds its graph from the edge
+ * list on every start). bingo_save writes the whole graph store (every slot,
+ * tombstone, group list, back-pointer, alias table and adjacency entry) to a
+ * file; bingo_restore replaces the handle's graph with a file's, so a
+ * restored handle walks and updates exactly like the one that saved it. The
+ * file is checksummed and tied to this build's record layout and to
+ * config.node2vec; a restore that fails leaves the handle with no graph. */
+int bingo_save(bingo_handle* h, const char* path);
+int bingo_restore(bingo_handle* h, const char* path);
+
 /* ---- Tuning -------------------------------------------------------------
  * Launch and batching parameters. None of them changes any result (walks,
  * slot ids, graph state); bingo_autotune picks them by measurement. */
