@@ -8,5 +8,5 @@ operator interface (`Graph.build / insert / deleteE / walk`).
 """
 from ._lib import BingoError, LIB_PATH, lib  # noqa: F401
 from .engine import (APPS, BATCHED, DEEPWALK, NODE2VEC, PLAIN, PPR, RUN_GRAPH, SAMPLING,  # noqa: F401
-                     WALK_PPR_TAIL, Graph, WalkJob)
+                     WALK_PPR_TAIL, Graph, WalkJob, fixed16)
 from . import gen  # noqa: F401

@@ -18,7 +18,7 @@ class BingoConfig(ctypes.Structure):
         ("device", c_int32),
         ("node2vec", c_uint32),
         ("synchronous", c_uint32),
-        ("reserved0", c_uint32),
+        ("weight_mode", c_uint32),
         ("arena_factor", c_double),
         ("arena_bytes", c_uint64),
     ]
@@ -106,7 +106,7 @@ class BingoServeMetrics(ctypes.Structure):
 class BingoStats(ctypes.Structure):
     _fields_ = [
         ("n", c_uint32),
-        ("reserved0", c_uint32),
+        ("weight_mode", c_uint32),
         ("slots", c_uint64),
         ("live_edges", c_uint64),
         ("arena_bytes", c_uint64),
@@ -128,6 +128,9 @@ SIGNATURES = {
     "bingo_insert_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
     "bingo_delete_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "bingo_delete_pairs": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
+    "bingo_load_edges_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_uint32]),
+    "bingo_insert_batch_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
+    "bingo_weights_to_fixed16": (c_uint64, [c_void_p, c_uint64, c_void_p]),
     "bingo_walk": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32, c_uint32]),
     "bingo_walk_noalloc": (c_int, [c_void_p, POINTER(BingoWalkJob), c_uint32]),
     "bingo_run": (c_int, [c_void_p, POINTER(BingoOp), c_uint32, c_uint32]),

@@ -1,5 +1,6 @@
 // extern "C" boundary: every entry point catches engine errors and returns a
 // bingo_status; the message stays readable through bingo_last_error().
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -66,6 +67,10 @@ int bingo_create(const bingo_config* cfg, bingo_handle** out) {
   bingo_config c;
   bingo_config_init(&c);
   if (cfg) c = *cfg;
+  if (c.weight_mode != BINGO_WEIGHTS_U32 && c.weight_mode != BINGO_WEIGHTS_F32) {
+    g_create_error = "unknown weight_mode";
+    return BINGO_ERR_INVALID_ARGUMENT;
+  }
   try {
     bingo_handle* h = new bingo_handle;
     h->device = c.device;
@@ -113,6 +118,28 @@ int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst
 
 int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot, uint64_t k) {
   return guarded(h, [&](bingo::Engine& e) { e.erase(u, slot, k); });
+}
+
+int bingo_load_edges_f32(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const float* w, uint64_t m,
+                         uint32_t n) {
+  return guarded(h, [&](bingo::Engine& e) { e.load_f32(src, dst, w, m, n); });
+}
+
+int bingo_insert_batch_f32(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const float* w, uint64_t k,
+                           uint32_t* out_slots) {
+  return guarded(h, [&](bingo::Engine& e) { e.insert_f32(src, dst, w, k, out_slots); });
+}
+
+uint64_t bingo_weights_to_fixed16(const float* w, uint64_t k, uint32_t* out) {
+  uint64_t bad = 0;
+  for (uint64_t i = 0; i < k; ++i) {
+    const float x = w[i];
+    uint32_t q = 0;
+    if (x > 0.0f && x < 65536.0f) q = (uint32_t)std::nearbyint(x * 65536.0f);  // default mode: half to even
+    bad += q == 0;
+    out[i] = q;
+  }
+  return bad;
 }
 
 int bingo_delete_pairs(bingo_handle* h, const uint32_t* u, const uint32_t* v, uint64_t k) {

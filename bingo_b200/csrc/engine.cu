@@ -170,6 +170,27 @@ __global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint
   }
 }
 
+// Float weights -> 16.16 fixed point, round half to even (the scaling by
+// 2^16 is exact in float). bad |= 1 for w <= 0, NaN or a weight that rounds
+// to 0; bad |= 2 for w >= 65536 (inf included).
+__global__ void k_fixed16(const float* w, unsigned long long k, uint32_t* out, uint32_t* bad) {
+  uint32_t bits = 0;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const float x = w[i];
+    uint32_t q = 0;
+    if (!(x > 0.0f))
+      bits |= 1u;
+    else if (!(x < 65536.0f))
+      bits |= 2u;
+    else if (!(q = __float2uint_rn(x * 65536.0f)))
+      bits |= 1u;
+    out[i] = q;
+  }
+  bits = __reduce_or_sync(kFull, bits);
+  if (bits && (threadIdx.x & 31) == 0) atomicOr(bad, bits);
+}
+
 // Delete by pair, step 1: 64-bit sort keys (u << 32) | v.
 __global__ void k_pair_keys(const uint32_t* u, const uint32_t* v, unsigned long long k, unsigned long long* key) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
@@ -850,6 +871,45 @@ void Engine::insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w,
   finish_call();
 }
 
+// Float-weight mode (bingo_load_edges_f32 / bingo_insert_batch_f32): the
+// weights become 16.16 fixed point on the device, then take the integer path.
+const uint32_t* Engine::fixed_weights(const float* w, uint64_t k) {
+  if (cfg_.weight_mode != BINGO_WEIGHTS_F32)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "float weights need a handle created with weight_mode = BINGO_WEIGHTS_F32");
+  if (!w) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null weight array");
+  const float* dw = w;
+  if (!is_device_ptr(w)) {
+    fw_in_.ensure(k * 4, "float weights");
+    cuda_check(cudaMemcpyAsync(fw_in_.p, w, k * 4, cudaMemcpyHostToDevice, stream_), "stage float weights");
+    dw = fw_in_.as<float>();
+  }
+  fw_fixed_.ensure(k * 4, "float weights");
+  ctl_.ensure(16, "scratch");
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 4, stream_), "ctl");
+  k_fixed16<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(dw, k, fw_fixed_.as<uint32_t>(), ctl_.as<uint32_t>());
+  cuda_check(cudaGetLastError(), "fixed-point weights");
+  ++launches_;
+  uint32_t bad = 0;
+  cuda_check(cudaMemcpyAsync(&bad, ctl_.p, 4, cudaMemcpyDeviceToHost, stream_), "read ctl");
+  cuda_check(cudaStreamSynchronize(stream_), "fixed-point weights");
+  if (bad & 2u) throw Error(BINGO_ERR_OUT_OF_RANGE, "float weight >= 65536 (the fixed-point range)");
+  if (bad & 1u) throw Error(BINGO_ERR_ZERO_WEIGHT, "float weight <= 0, NaN, or below 2^-17 (rounds to 0)");
+  return fw_fixed_.as<uint32_t>();
+}
+
+void Engine::load_f32(const uint32_t* src, const uint32_t* dst, const float* w, uint64_t m, uint32_t n) {
+  if (m >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 edges in one load");
+  const uint32_t* q = m ? fixed_weights(w, m) : nullptr;
+  load(src, dst, m ? q : nullptr, m, n);
+  fw_in_.release(), fw_fixed_.release();
+}
+
+void Engine::insert_f32(const uint32_t* src, const uint32_t* dst, const float* w, uint64_t k, uint32_t* out_slots) {
+  if (k == 0) return;
+  if (k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 edges in one batch");
+  insert(src, dst, fixed_weights(w, k), k, out_slots);
+}
+
 // Rejects the batch (status, nothing applied) when a device-resident column
 // holds an id >= n or a zero weight; host columns are checked on the host.
 void Engine::check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k) {
@@ -1495,6 +1555,7 @@ void Engine::philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, ui
 void Engine::stats(bingo_stats* out) {
   std::memset(out, 0, sizeof *out);
   out->n = n_;
+  out->weight_mode = cfg_.weight_mode;
   if (server_) {  // the scheduler owns the stream and the host mirrors
     cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
     out->kernel_launches = launches_;

@@ -65,6 +65,8 @@ class Engine {
 
   void load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n);
   void insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
+  void load_f32(const uint32_t* src, const uint32_t* dst, const float* w, uint64_t m, uint32_t n);
+  void insert_f32(const uint32_t* src, const uint32_t* dst, const float* w, uint64_t k, uint32_t* out_slots);
   void erase(const uint32_t* u, const uint32_t* slot, uint64_t k);
   void erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k);
   void walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
@@ -123,6 +125,7 @@ class Engine {
   DevBuf in_a_, in_b_, in_c_, key_s_, perm_, iota_, sa_, sb_, head_, seg_, nseg_, need_, scan_, base_, ctl_,
       slots_, cub_tmp_;
   DevBuf pair_key_, pair_key_s_, pair_slot_;  // delete-by-pair translation
+  DevBuf fw_in_, fw_fixed_;                   // float weights: staged input, 16.16 fixed point
   uint64_t iota_n_ = 0;
   // walk scratch
   DevBuf jobs_, prefix_, queue_, wstart_, wout_;
@@ -152,6 +155,7 @@ class Engine {
   void require_loaded() const;
   void insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
   void erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k);
+  const uint32_t* fixed_weights(const float* w, uint64_t k);
   void check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k);
   bool save_state(StateCopy& c);
   void restore_state(const StateCopy& c);

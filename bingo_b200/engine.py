@@ -26,6 +26,30 @@ OP_WALK, OP_INSERT, OP_DELETE = 0, 1, 2
 RUN_GRAPH = 1
 
 
+def _is_float(a) -> bool:
+    if hasattr(a, "dtype") and hasattr(a, "data_ptr"):
+        return a.dtype.is_floating_point
+    return np.asarray(a).dtype.kind == "f"
+
+
+def _f32(a):
+    """Pointer + keep-alive for a float32 array (numpy host array or CUDA tensor)."""
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous() or a.element_size() != 4:
+            raise ValueError("expected a contiguous float32 tensor")
+        return ctypes.c_void_p(a.data_ptr()), a
+    arr = np.ascontiguousarray(a, dtype=np.float32)
+    return ctypes.c_void_p(arr.ctypes.data), arr
+
+
+def fixed16(w) -> np.ndarray:
+    """Float weights -> the float-weight mode's 16.16 fixed point (bingo_weights_to_fixed16); invalid -> 0."""
+    arr = np.ascontiguousarray(w, dtype=np.float32)
+    out = np.empty(len(arr), np.uint32)
+    lib().bingo_weights_to_fixed16(ctypes.c_void_p(arr.ctypes.data), len(arr), ctypes.c_void_p(out.ctypes.data))
+    return out
+
+
 def _u32(a):
     """Pointer + keep-alive for a uint32 array (numpy host array or CUDA tensor)."""
     if a is None:
@@ -69,11 +93,13 @@ class Graph:
     """A dynamic weighted graph resident on one GPU."""
 
     def __init__(self, device: int = 0, node2vec: bool = True, synchronous: bool = True,
-                 arena_factor: float = 2.0, arena_bytes: int = 0):
+                 arena_factor: float = 2.0, arena_bytes: int = 0, float_weights: bool = False):
         L = lib()
         cfg = BingoConfig()
         L.bingo_config_init(ctypes.byref(cfg))
         cfg.device = device
+        cfg.weight_mode = 1 if float_weights else 0
+        self.float_weights = float_weights
         cfg.node2vec = 1 if node2vec else 0
         cfg.synchronous = 1 if synchronous else 0
         cfg.arena_factor = arena_factor
@@ -117,9 +143,13 @@ class Graph:
         """Load a graph (reference build(), include/operation.cuh:33)."""
         ps, ks = _u32(src)
         pd, kd = _u32(dst)
-        pw, kw = _u32(w)
         m = len(src) if not hasattr(src, "numel") else src.numel()
-        self._check(self._L.bingo_load_edges(self._h, ps, pd, pw, m, n))
+        if _is_float(w):  # float weights (handle created with float_weights=True)
+            pw, kw = _f32(w)
+            self._check(self._L.bingo_load_edges_f32(self._h, ps, pd, pw, m, n))
+        else:
+            pw, kw = _u32(w)
+            self._check(self._L.bingo_load_edges(self._h, ps, pd, pw, m, n))
         self.n = n
 
     def insert_batch(self, src, dst, w, out_slots=None, return_slots: bool = True):
@@ -128,11 +158,15 @@ class Graph:
         k = len(src) if not hasattr(src, "numel") else src.numel()
         ps, ks = _u32(src)
         pd, kd = _u32(dst)
-        pw, kw = _u32(w)
         if out_slots is None and return_slots:
             out_slots = np.empty(k, dtype=np.uint32)
         po, ko = _out(out_slots, np.uint32) if out_slots is not None else (None, None)
-        self._check(self._L.bingo_insert_batch(self._h, ps, pd, pw, k, po))
+        if _is_float(w):
+            pw, kw = _f32(w)
+            self._check(self._L.bingo_insert_batch_f32(self._h, ps, pd, pw, k, po))
+        else:
+            pw, kw = _u32(w)
+            self._check(self._L.bingo_insert_batch(self._h, ps, pd, pw, k, po))
         return out_slots
 
     def delete_batch(self, u, slot):

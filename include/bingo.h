@@ -58,11 +58,22 @@ typedef enum bingo_app {
 #define BINGO_WALK_BATCHED 0u /* all jobs in one persistent launch over a device work queue */
 #define BINGO_WALK_PLAIN 1u   /* one launch per job, the reference's per-job form */
 
+/* Weight modes. U32: integer weights >= 1 (the reference's wtype::Int).
+ * F32: float weights in (0, 65536) (the reference's wtype::Float, whose
+ * integer part is limited to MAXLOG = 16 bits, include/api.h:11), kept as
+ * 16.16 fixed point q = round_half_even(w * 2^16): every kernel then runs
+ * unchanged and draws exactly in proportion to q, so each probability is
+ * within 2^-17 / w relative of the float weight's. In F32 mode every uint32
+ * weight the API takes or returns (bingo_run, serving updates, dumps) is such
+ * a fixed-point value; bingo_weights_to_fixed16 converts. */
+#define BINGO_WEIGHTS_U32 0
+#define BINGO_WEIGHTS_F32 1
+
 typedef struct bingo_config {
   int32_t device;         /* CUDA device ordinal */
   uint32_t node2vec;      /* maintain the adjacency index node2vec needs (like NODE2VEC, include/api.h:25) */
   uint32_t synchronous;   /* 1: every call waits for its device work (default) */
-  uint32_t reserved0;
+  uint32_t weight_mode;   /* BINGO_WEIGHTS_U32 (default) or BINGO_WEIGHTS_F32 */
   double arena_factor;    /* graph arena = factor x bytes needed at load (default 2.0) */
   uint64_t arena_bytes;   /* minimum graph arena bytes; 0 = from arena_factor only */
 } bingo_config;
@@ -86,7 +97,7 @@ typedef struct bingo_walk_job {
 
 typedef struct bingo_stats {
   uint32_t n;             /* vertices */
-  uint32_t reserved0;
+  uint32_t weight_mode;   /* the handle's BINGO_WEIGHTS_* */
   uint64_t slots;         /* edge slots including tombstones */
   uint64_t live_edges;
   uint64_t arena_bytes;   /* bytes reserved for the graph arenas */
@@ -127,6 +138,23 @@ int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst
  * batch order; a slot that is absent or already deleted is skipped and the
  * call returns BINGO_ERR_INVALID_SLOT after applying the rest. */
 int bingo_delete_batch(bingo_handle* h, const uint32_t* u, const uint32_t* slot, uint64_t k);
+
+/* Float-weight forms of bingo_load_edges / bingo_insert_batch for handles
+ * created with weight_mode = BINGO_WEIGHTS_F32 (the reference's
+ * wtype::Float load and insert, include/Bingo.cuh:65-69, :176-177, :189-190).
+ * The reference keeps the fractional parts as one remainder group drawn by
+ * rejection over all slots (include/Bingo.cuh:254-264); here the weight is
+ * quantised to 16.16 fixed point and lands in the bit groups like any other.
+ * A weight that is not in (0, 65536), or that rounds to 0 (w < 2^-17),
+ * rejects the whole batch (BINGO_ERR_ZERO_WEIGHT for w <= 0, NaN or w
+ * rounding to 0; BINGO_ERR_OUT_OF_RANGE for w >= 65536). */
+int bingo_load_edges_f32(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const float* w, uint64_t m,
+                         uint32_t n);
+int bingo_insert_batch_f32(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const float* w, uint64_t k,
+                           uint32_t* out_slots);
+/* Host conversion to the F32 mode's fixed point (same rounding as the
+ * device); invalid weights become 0. Returns the number of invalid weights. */
+uint64_t bingo_weights_to_fixed16(const float* w, uint64_t k, uint32_t* out);
 
 /* Delete by (u, v) pair; no reference counterpart (the reference deletes by
  * slot only, include/operation.cuh:215). The r-th occurrence of a pair in the
