@@ -601,7 +601,10 @@ def measure_engine(args, n, src, dst, w, batches, local):
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-    g = Graph(device=local, synchronous=False)
+    # DeepWalk only: no node2vec adjacency index, as the reference builds it
+    # only for node2vec runs (NODE2VEC = 0 unless the app is node2vec,
+    # include/api.h:26, src/apps.cu:14-15).
+    g = Graph(device=local, synchronous=False, node2vec=False)
     g.set_stream(stream.cuda_stream)
     g.load_edges(src, dst, w, n)
 
@@ -653,7 +656,10 @@ def run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world):
         return t
 
     hbatches = [((pinned(i[0]), pinned(i[1]), pinned(i[2])), (pinned(d[0]), pinned(d[1]))) for i, d in batches]
-    hout = torch.empty((n, WALK_LEN), dtype=torch.int32).pin_memory()
+    # Two host result buffers used in turn (a consumer reads one step's rows
+    # while the next step runs); the engine copies each step's rows out while
+    # the next step's kernels run, and bingo_sync waits for the copies.
+    hout = [torch.empty((n, WALK_LEN), dtype=torch.int32).pin_memory() for _ in range(2)]
     hslots = torch.empty(BATCH_INS, dtype=torch.int32).pin_memory()
 
     def e2e_step(i):
@@ -661,7 +667,7 @@ def run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world):
         g.insert_batch(a, b, c, out_slots=hslots)
         g.delete_batch(du, ds)
         g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, starts=None, n_starts=n, first=0, job_id=i, seed=seed,
-                             out=hout)], mode=PLAIN)
+                             out=hout[i % 2])], mode=PLAIN)
 
     for i in range(args.warmup):
         e2e_step(i)
@@ -674,6 +680,7 @@ def run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world):
     e0.record(stream)
     for i in range(args.warmup, total):
         e2e_step(i)
+    g.sync()  # every result copy has landed in host memory
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier(world)
@@ -706,7 +713,10 @@ def run_ours(args):
     # A dedicated (non-default) stream shared by torch's events and the engine.
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-    g = Graph(device=local, synchronous=False)
+    # DeepWalk only: no node2vec adjacency index, as the reference builds it
+    # only for node2vec runs (NODE2VEC = 0 unless the app is node2vec,
+    # include/api.h:26, src/apps.cu:14-15).
+    g = Graph(device=local, synchronous=False, node2vec=False)
     g.set_stream(stream.cuda_stream)
     g.load_edges(src, dst, w, n)
     g.sync()

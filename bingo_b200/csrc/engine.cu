@@ -117,6 +117,17 @@ __global__ void k_totals(const unsigned long long* need, const unsigned long lon
 }
 
 // All-or-nothing reservation of the batch's arena space.
+// Publishes the insert plan to mapped host memory: out[0..5) totals,
+// out[5] the batch status word, out[6..11) the arena tops.
+__global__ void k_publish_plan(const unsigned long long* tot, const uint32_t* ctl, const unsigned long long* top,
+                               volatile unsigned long long* out) {
+  const int t = threadIdx.x;
+  if (t < kArenas) out[t] = tot[t];
+  if (t == kArenas) out[kArenas] = *ctl;
+  if (t < kArenas) out[kArenas + 1 + t] = top[t];
+  __threadfence_system();
+}
+
 __global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base) {
   if (threadIdx.x || blockIdx.x || *ctl) return;
   bool ok = true;
@@ -518,6 +529,11 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
   cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
   cuda_check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   stream_ = own_stream_;
+  cuda_check(cudaStreamCreateWithFlags(&xstream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int k = 0; k < 2; ++k) {
+    cuda_check(cudaEventCreateWithFlags(&walk_ev_[k], cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaEventCreateWithFlags(&copy_ev_[k], cudaEventDisableTiming), "cudaEventCreate");
+  }
   cuda_check(cudaMalloc(&d_err_, 4 * sizeof(uint32_t)), "cudaMalloc(err)");
   cuda_check(cudaMemset(d_err_, 0, 4 * sizeof(uint32_t)), "memset(err)");
   cuda_check(cudaMalloc(&d_top_, kArenas * sizeof(unsigned long long)), "cudaMalloc(top)");
@@ -527,18 +543,30 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
   cuda_check(cudaMallocHost(&h_err_, 4 * sizeof(uint32_t)), "cudaMallocHost(err)");
   cuda_check(cudaMallocHost(&h_top_, kArenas * sizeof(unsigned long long)), "cudaMallocHost(top)");
   std::memset(h_top_, 0, kArenas * sizeof(unsigned long long));
+  cuda_check(cudaHostAlloc((void**)&h_plan_, 16 * sizeof(unsigned long long), cudaHostAllocMapped),
+             "cudaHostAlloc(plan)");
+  cuda_check(cudaHostGetDevicePointer((void**)&d_plan_, (void*)h_plan_, 0), "plan mapping");
+  cuda_check(cudaEventCreateWithFlags(&slots_ev_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Engine::~Engine() {
   cudaSetDevice(cfg_.device);
   server_.reset();
   if (stream_) cudaStreamSynchronize(stream_);
+  if (xstream_) cudaStreamSynchronize(xstream_);
   drop_graph();
   prog_jobs_.release(), prog_prefix_.release(), prog_queue_.release();
   DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
                     &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
-                    &prefix_, &queue_, &wstart_, &wout_, &pair_key_, &pair_key_s_, &pair_slot_};
+                    &prefix_, &queue_, &wstart_, &wout_[0], &wout_[1], &pair_key_, &pair_key_s_, &pair_slot_};
   for (DevBuf* b : bufs) b->release();
+  for (int k = 0; k < 2; ++k) {
+    if (walk_ev_[k]) cudaEventDestroy(walk_ev_[k]);
+    if (copy_ev_[k]) cudaEventDestroy(copy_ev_[k]);
+  }
+  if (xstream_) cudaStreamDestroy(xstream_);
+  if (slots_ev_) cudaEventDestroy(slots_ev_);
+  if (h_plan_) cudaFreeHost((void*)h_plan_);
   for (auto& a : arena_) a.release();
   if (d_err_) cudaFree(d_err_);
   if (d_top_) cudaFree(d_top_);
@@ -587,6 +615,7 @@ void Engine::set_stream(void* s) { stream_ = s ? (cudaStream_t)s : own_stream_; 
 
 int Engine::sync() {
   cuda_check(cudaStreamSynchronize(stream_), "stream synchronize");
+  cuda_check(cudaStreamSynchronize(xstream_), "result copies");
   cuda_check(cudaMemcpy(h_err_, d_err_, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost), "read status");
   const uint32_t bits = h_err_[0], rejected = h_err_[1];
   if (!bits) return BINGO_OK;
@@ -608,6 +637,10 @@ void Engine::finish_call() {
 // ------------------------------------------------------------------ staging
 void Engine::ensure_batch_scratch(uint64_t k) {
   const uint64_t kk = std::max<uint64_t>(k, 1);
+  if (slots_busy_ && slots_.bytes < kk * 4) {  // slots_ is about to move: its copy-out must be over
+    cuda_check(cudaEventSynchronize(slots_ev_), "slot copy");
+    slots_busy_ = false;
+  }
   const uint64_t ks = std::max<uint64_t>(std::min<uint64_t>(kk, n_ ? n_ : kk), 1);
   in_a_.ensure(kk * 4, "scratch");
   in_b_.ensure(kk * 4, "scratch");
@@ -756,14 +789,15 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   k_totals<<<1, 32, 0, stream_>>>(need_.as<unsigned long long>(), scan_.as<unsigned long long>(), ks, d_tot);
   cuda_check(cudaGetLastError(), "totals");
   ++launches_;
-  unsigned long long tot[kArenas];
-  uint32_t ctl = 0;
-  cuda_check(cudaMemcpyAsync(tot, d_tot, sizeof tot, cudaMemcpyDeviceToHost, stream_), "read totals");
-  cuda_check(cudaMemcpyAsync(&ctl, ctl_.p, 4, cudaMemcpyDeviceToHost, stream_), "read ctl");
-  if (!load_mode)
-    cuda_check(cudaMemcpyAsync(h_top_, d_top_, kArenas * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
-               "read tops");
+  k_publish_plan<<<1, 32, 0, stream_>>>(d_tot, ctl_.as<uint32_t>(), d_top_, d_plan_);
+  cuda_check(cudaGetLastError(), "publish plan");
+  ++launches_;
   cuda_check(cudaStreamSynchronize(stream_), "plan sync");
+  unsigned long long tot[kArenas];
+  for (int a = 0; a < kArenas; ++a) tot[a] = h_plan_[a];
+  const uint32_t ctl = (uint32_t)h_plan_[kArenas];
+  if (!load_mode)
+    for (int a = 0; a < kArenas; ++a) h_top_[a] = h_plan_[kArenas + 1 + a];
   if (ctl) {
     cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
     const int st = status_of(ctl);
@@ -933,6 +967,13 @@ void Engine::check_batch_on_device(const uint32_t* a, const uint32_t* b, const u
 }
 
 void Engine::insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots) {
+  if (slots_busy_) {  // the last host-bound slot copy reads slots_: finish it before slots_ changes
+    if (slots_.bytes < std::max<uint64_t>(k, 1) * 4)
+      cuda_check(cudaEventSynchronize(slots_ev_), "slot copy");
+    else
+      cuda_check(cudaStreamWaitEvent(stream_, slots_ev_, 0), "slot copy");
+    slots_busy_ = false;
+  }
   ensure_batch_scratch(k);
   const uint32_t* ds = stage(src, k, in_a_, "stage src");
   const uint32_t* dd = stage(dst, k, in_b_, "stage dst");
@@ -945,8 +986,18 @@ void Engine::insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t
   const bool dev_out = out_slots && is_device_ptr(out_slots);
   uint32_t* dslots = out_slots ? (dev_out ? out_slots : slots_.as<uint32_t>()) : nullptr;
   run_insert(k, dslots, false, k);
-  if (out_slots && !dev_out)
-    cuda_check(cudaMemcpyAsync(out_slots, dslots, k * 4, cudaMemcpyDeviceToHost, stream_), "slots D2H");
+  if (out_slots && !dev_out) {
+    if (cfg_.synchronous) {
+      cuda_check(cudaMemcpyAsync(out_slots, dslots, k * 4, cudaMemcpyDeviceToHost, stream_), "slots D2H");
+    } else {
+      // Copied out beside the walk results; bingo_sync waits for it.
+      cuda_check(cudaEventRecord(slots_ev_, stream_), "slots ready");
+      cuda_check(cudaStreamWaitEvent(xstream_, slots_ev_, 0), "slots ready");
+      cuda_check(cudaMemcpyAsync(out_slots, dslots, k * 4, cudaMemcpyDeviceToHost, xstream_), "slots D2H");
+      cuda_check(cudaEventRecord(slots_ev_, xstream_), "slots copied");
+      slots_busy_ = true;
+    }
+  }
 }
 
 void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
@@ -1071,7 +1122,22 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     prefix[j + 1] = prefix[j] + J.n_starts;
   }
   if (s_total) wstart_.ensure(s_total * 4, "walk staging");
-  if (o_total) wout_.ensure(o_total * 4, "walk staging");
+  // Host-bound outputs go through the next staging buffer; its previous
+  // copy-out must finish before these kernels overwrite it (a device-side
+  // wait, no host synchronisation).
+  int32_t* wout = nullptr;
+  const int ring = wout_next_;
+  if (o_total) {
+    wout_next_ ^= 1;
+    if (wout_busy_[ring]) {
+      if (wout_[ring].bytes < o_total * 4)  // about to reallocate: its copy-out must be over first
+        cuda_check(cudaEventSynchronize(copy_ev_[ring]), "staging reuse");
+      else
+        cuda_check(cudaStreamWaitEvent(stream_, copy_ev_[ring], 0), "staging reuse");
+    }
+    wout_[ring].ensure(o_total * 4, "walk staging");
+    wout = wout_[ring].as<int32_t>();
+  }
   for (uint32_t j = 0; j < n_jobs; ++j) {
     const bingo_walk_job& J = jobs[j];
     WalkJobDev& D = dj[j];
@@ -1082,7 +1148,7 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
       cuda_check(cudaMemcpyAsync(d, J.starts, J.n_starts * 4, cudaMemcpyHostToDevice, stream_), "starts H2D");
       D.starts = d;
     }
-    D.out = o_off[j] != ~0ull ? wout_.as<int32_t>() + o_off[j] : J.out;
+    D.out = o_off[j] != ~0ull ? wout + o_off[j] : J.out;
   }
   if (mode == BINGO_WALK_BATCHED && prefix[n_jobs] >= (1ull << 32))
     throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^32 walks in one batched call");
@@ -1150,13 +1216,25 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
       ++launches_;
     }
   }
-  for (uint32_t j = 0; j < n_jobs; ++j)
-    if (o_off[j] != ~0ull) {
-      const uint64_t per = jobs[j].app == BINGO_SAMPLING ? 1 : jobs[j].length;
-      cuda_check(cudaMemcpyAsync(jobs[j].out, wout_.as<int32_t>() + o_off[j], jobs[j].n_starts * per * 4,
-                                 cudaMemcpyDeviceToHost, stream_),
-                 "walk D2H");
+  if (o_total) {
+    // Asynchronous handles copy out on xstream_, after this call's kernels;
+    // the next call's kernels proceed meanwhile. bingo_sync waits for both.
+    cudaStream_t cs = stream_;
+    if (!cfg_.synchronous) {
+      cs = xstream_;
+      cuda_check(cudaEventRecord(walk_ev_[ring], stream_), "walk done");
+      cuda_check(cudaStreamWaitEvent(xstream_, walk_ev_[ring], 0), "copy after walk");
     }
+    for (uint32_t j = 0; j < n_jobs; ++j)
+      if (o_off[j] != ~0ull) {
+        const uint64_t per = jobs[j].app == BINGO_SAMPLING ? 1 : jobs[j].length;
+        cuda_check(cudaMemcpyAsync(jobs[j].out, wout + o_off[j], jobs[j].n_starts * per * 4, cudaMemcpyDeviceToHost,
+                                   cs),
+                   "walk D2H");
+      }
+    cuda_check(cudaEventRecord(copy_ev_[ring], cs), "copy done");
+    wout_busy_[ring] = true;
+  }
   finish_call();
 }
 
@@ -1575,7 +1653,7 @@ void Engine::stats(bingo_stats* out) {
   }
   const DevBuf* sc[] = {&in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_, &sb_, &head_, &seg_, &nseg_,
                         &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_, &prefix_, &queue_, &wstart_,
-                        &wout_};
+                        &wout_[0], &wout_[1]};
   for (const DevBuf* b : sc) out->scratch_bytes += b->bytes;
 }
 

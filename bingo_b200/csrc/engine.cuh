@@ -118,6 +118,13 @@ class Engine {
   uint32_t* d_err_ = nullptr;            // [0] ErrBit sticky, [1] rejected deletes
   uint32_t* h_err_ = nullptr;            // pinned mirror
   unsigned long long* h_top_ = nullptr;  // pinned mirror of d_top_
+  // Insert plan read-back (totals, status, tops) through mapped host memory,
+  // written by a kernel: no copy-engine transfer that could queue behind a
+  // large result copy.
+  volatile unsigned long long* h_plan_ = nullptr;
+  unsigned long long* d_plan_ = nullptr;
+  cudaEvent_t slots_ev_ = nullptr;  // host-bound slot ids copied out (asynchronous handles)
+  bool slots_busy_ = false;
   unsigned long long* d_steps_ = nullptr;  // produced walk steps since create
   unsigned long long launches_ = 0;        // hand-written kernels launched since create
 
@@ -128,7 +135,15 @@ class Engine {
   DevBuf fw_in_, fw_fixed_;                   // float weights: staged input, 16.16 fixed point
   uint64_t iota_n_ = 0;
   // walk scratch
-  DevBuf jobs_, prefix_, queue_, wstart_, wout_;
+  DevBuf jobs_, prefix_, queue_, wstart_;
+  // Host-bound walk outputs: two device staging buffers used in turn; each
+  // is copied out on xstream_ (asynchronous handles), so one call's copy-out
+  // overlaps the next call's kernels. copy_ev_[k] marks buffer k's copy done.
+  DevBuf wout_[2];
+  cudaStream_t xstream_ = nullptr;
+  cudaEvent_t walk_ev_[2] = {nullptr, nullptr}, copy_ev_[2] = {nullptr, nullptr};
+  bool wout_busy_[2] = {false, false};
+  int wout_next_ = 0;
   // programs
   DevBuf prog_jobs_, prog_prefix_, prog_queue_;
   cudaGraph_t graph_ = nullptr;

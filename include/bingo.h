@@ -12,7 +12,9 @@
  * ordered on the handle's CUDA stream. With cfg.synchronous != 0 (the
  * default) each call returns only after its device work is complete and
  * reports device-detected errors directly; otherwise such errors surface at
- * the next bingo_sync().
+ * the next bingo_sync(), and walk rows bound for host memory are complete
+ * only after it: they are copied out on a second stream while the next
+ * calls' device work runs.
  *
  * Threading: one handle may be used by one host thread at a time.
  */
