@@ -554,19 +554,23 @@ def run_reference_cuda(args):
         return
     total = args.warmup + args.steps
     w_hi = 1 << 16
-    n, src, dst, w, batches = make_workload(total, w_hi=w_hi)
+    n2v = args.workload == "node2vec"
+    if n2v:  # config 3 with the reference's limits: weights < 2^16 (MAXLOG), its fixed LEN = 80, p = 0.5, q = 2
+        n, src, dst, w, batches = make_node2vec_workload(total, w_hi=w_hi - 1)
+    else:
+        n, src, dst, w, batches = make_workload(total, w_hi=w_hi)
     with tempfile.TemporaryDirectory() as td:
         inp = os.path.join(td, "in.bin")
         with open(inp, "wb") as f:
             f.write(b"BREF")
-            f.write(struct.pack("<IIQfI", 1, n, len(src), 0.4, 0))
+            f.write(struct.pack("<IIQfI", 1, n, len(src), 0.4, 1 if n2v else 0))
             f.write(np.stack([src, dst, w], 1).astype("<u4").tobytes())
             for i, (ins, dels) in enumerate(batches):
                 f.write(struct.pack("<IQ", 1, len(ins[0])))
                 f.write(np.stack(ins, 1).astype("<u4").tobytes())
                 f.write(struct.pack("<IQ", 2, len(dels[0])))
                 f.write(np.stack(dels, 1).astype("<u4").tobytes())
-                f.write(struct.pack("<IIIQ", 4, 0, 1, 1000 + i))
+                f.write(struct.pack("<IIIQ", 4, 1 if n2v else 0, 1, 1000 + i))
             f.write(struct.pack("<I", 0))
         r = subprocess.run([REF_HARNESS, inp, "-"], capture_output=True, text=True, timeout=1800)
     if r.returncode:
@@ -579,32 +583,45 @@ def run_reference_cuda(args):
     walks = [o for o in ops if o["op"] == "walk"][args.warmup:]
     walk_s = sum(o["kernel_ms"] for o in walks) / 1e3
     steps = sum(o["steps"] for o in walks)
+    upd_per_step = sum(len(b[0][0]) + len(b[1][0]) for b in batches[args.warmup:]) / max(len(walks), 1)
     ref = {"value": steps / (walk_s + sum(ins_s) + sum(del_s)), "walk_steps_per_s": steps / walk_s,
-           "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * len(walks) / (sum(ins_s) + sum(del_s)),
+           "edge_updates_per_s": upd_per_step * len(walks) / (sum(ins_s) + sum(del_s)),
            "walk_kernel_ms_per_step": walk_s * 1e3 / len(walks),
            "update_wall_ms_per_step": (sum(ins_s) + sum(del_s)) * 1e3 / len(walks),
            "steps_per_walk_phase": steps / len(walks)}
-    ours = measure_engine(args, n, src, dst, w, batches, local)
+    if n2v:
+        from bingo_b200 import NODE2VEC
+        ours = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=WALK_LEN, p=0.5, q=2.0)
+        cfg = {"workload": "plain-node2vec-rmat22-w16", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
+               "weights": "zipf(1.2)[1,2^16)", "walks": n, "walk_len": WALK_LEN, "p": 0.5, "q": 2.0,
+               "batch": {"insert": N_BATCH // 2, "delete": N_BATCH // 2},
+               "note": "walk length 80 = the reference's compile-time LEN (include/api.h:12); its node2vec tests "
+                       "prev in N(cur) with a load-time hash (include/operation.cuh:313), so its step counts "
+                       "and acceptance differ from the exact node2vec here"}
+    else:
+        ours = measure_engine(args, n, src, dst, w, batches, local)
+        cfg = {"workload": WORKLOAD + "-w16", "scale": SCALE, "edge_factor": EDGE_FACTOR,
+               "weights": "loguniform[1,2^16)", "walks": n, "walk_len": WALK_LEN,
+               "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}}
     line = {"impl": "reference-cuda", "metric": "walk_steps_per_s", "value": ref["value"], "unit": "steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "config": {"workload": WORKLOAD + "-w16", "scale": SCALE, "edge_factor": EDGE_FACTOR,
-                       "weights": "loguniform[1,2^16)", "walks": n, "walk_len": WALK_LEN,
-                       "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}},
-            "reference": ref, "ours_same_input": ours}
+            "config": cfg, "reference": ref, "ours_same_input": ours}
     print(json.dumps(line), flush=True)
 
 
-def measure_engine(args, n, src, dst, w, batches, local):
-    """This engine on the given workload: device-timed steps (inputs in HBM)."""
+def measure_engine(args, n, src, dst, w, batches, local, app=None, length=WALK_LEN, p=0.5, q=2.0):
+    """This engine on the given workload: device-timed steps (inputs in HBM).
+    app None = DeepWalk."""
     import torch
-    from bingo_b200 import DEEPWALK, PLAIN, Graph, WalkJob
+    from bingo_b200 import DEEPWALK, NODE2VEC, PLAIN, Graph, WalkJob
+    app = DEEPWALK if app is None else app
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-    # DeepWalk only: no node2vec adjacency index, as the reference builds it
-    # only for node2vec runs (NODE2VEC = 0 unless the app is node2vec,
+    # The node2vec adjacency index only for node2vec, as the reference builds
+    # it only for node2vec runs (NODE2VEC = 0 unless the app is node2vec,
     # include/api.h:26, src/apps.cu:14-15).
-    g = Graph(device=local, synchronous=False, node2vec=False)
+    g = Graph(device=local, synchronous=False, node2vec=(app == NODE2VEC))
     g.set_stream(stream.cuda_stream)
     g.load_edges(src, dst, w, n)
 
@@ -612,33 +629,90 @@ def measure_engine(args, n, src, dst, w, batches, local):
         return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)
 
     db = [((dev_i32(i[0]), dev_i32(i[1]), dev_i32(i[2])), (dev_i32(d[0]), dev_i32(d[1]))) for i, d in batches]
-    out = torch.empty((n, WALK_LEN), dtype=torch.int32, device=dev)
-    slots = torch.empty(BATCH_INS, dtype=torch.int32, device=dev)
+    out = torch.empty((n, length), dtype=torch.int32, device=dev)
+    slots = torch.empty(max(len(b[0][0]) for b in batches), dtype=torch.int32, device=dev)
     total = args.warmup + args.steps
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(total)]
+    upd_edges = 0
     for i in range(total):
         if i == args.warmup:
             g.sync()
-            s0 = g.stats()["walk_steps"]
+            s0 = g.stats()
         (a, b, c), (du, ds) = db[i]
+        if i >= args.warmup:
+            upd_edges += a.numel() + du.numel()
         ev[i][0].record(stream)
-        g.insert_batch(a, b, c, out_slots=slots)
+        g.insert_batch(a, b, c, out_slots=slots[:a.numel()])
         g.delete_batch(du, ds)
         ev[i][1].record(stream)
-        g.walk_jobs([WalkJob(app=DEEPWALK, length=WALK_LEN, n_starts=n, first=0, job_id=i, seed=1, out=out)],
+        g.walk_jobs([WalkJob(app=app, length=length, n_starts=n, first=0, job_id=i, seed=1, p=p, q=q, out=out)],
                     mode=PLAIN)
         ev[i][2].record(stream)
     g.sync()
     torch.cuda.synchronize(dev)
-    steps = g.stats()["walk_steps"] - s0
+    s1 = g.stats()
+    steps = s1["walk_steps"] - s0["walk_steps"]
     upd = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(args.warmup, total)) / 1e3
     wlk = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
     whole = sum(ev[i][0].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
     g.close()
-    return {"value": steps / whole, "walk_steps_per_s": steps / wlk,
-            "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * args.steps / upd,
-            "walk_kernel_ms_per_step": wlk * 1e3 / args.steps, "update_ms_per_step": upd * 1e3 / args.steps,
-            "steps_per_walk_phase": steps / args.steps}
+    r = {"value": steps / whole, "walk_steps_per_s": steps / wlk, "edge_updates_per_s": upd_edges / upd,
+         "walk_kernel_ms_per_step": wlk * 1e3 / args.steps, "update_ms_per_step": upd * 1e3 / args.steps,
+         "steps_per_walk_phase": steps / args.steps}
+    if app == NODE2VEC:
+        trials = s1["walk_trials"] - s0["walk_trials"]
+        probes = s1["walk_probes"] - s0["walk_probes"]
+        r.update(trials_per_step=trials / max(steps, 1), probes_per_step=probes / max(steps, 1),
+                 algorithmic_gbs=(trials * N2V_BYTES_PER_TRIAL + probes * N2V_BYTES_PER_PROBE) / wlk / 1e9)
+    return r
+
+
+# --------------------------------------------------------------------------- node2vec (config 3)
+N_SCALE, N_LEN, N_BATCH = 22, 40, 1_000_000
+N_SEED = 1234 + 3
+N2V_BYTES_PER_TRIAL, N2V_BYTES_PER_PROBE = 32, 8  # algorithmic bytes: one alias draw; one adjacency lookup
+
+
+def make_node2vec_workload(steps_total: int, w_hi: int = (1 << 24) - 1):
+    """R-MAT scale 22 (edge factor 16), Zipf(s = 1.2) weights on [1, w_hi];
+    per step one update batch of 1M edges (500K absent-pair inserts + 500K
+    uniform live-edge deletes) then one node2vec walk per vertex."""
+    from bingo_b200 import gen
+    n = 1 << N_SCALE
+    src, dst = gen.rmat(N_SCALE, EDGE_FACTOR, seed=N_SEED)
+    w = gen.weights(len(src), gen.W_ZIPF, 1, w_hi, 1.2, seed=N_SEED + 1)
+    ug = gen.UpdateGen(n, src, dst, seed=N_SEED + 2)
+    batches = [(ug.inserts(N_BATCH // 2, gen.W_ZIPF, 1, w_hi, 1.2), ug.deletes(N_BATCH // 2))
+               for _ in range(steps_total)]
+    return n, src, dst, w, batches
+
+
+def run_node2vec(args):
+    """Config 3 in the plain per-job form: node2vec (p = 0.5, q = 2) walks of
+    length 40 from every vertex of an R-MAT scale 22 graph with Zipf weights,
+    after each 1M-edge update batch; device-timed, inputs in HBM."""
+    from bingo_b200 import NODE2VEC
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    total = args.warmup + args.steps
+    n, src, dst, w, batches = make_node2vec_workload(total)
+    r = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=N_LEN, p=0.5, q=2.0)
+    peak, peak_src = peak_hbm()
+    line = {"metric": "walk_steps_per_s", "value": r["value"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (r["walk_kernel_ms_per_step"] + r["update_ms_per_step"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "plain-node2vec-rmat22", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
+                       "m": int(len(src)), "weights": "zipf(1.2)[1,2^24)", "walks": n, "walk_len": N_LEN, "p": 0.5,
+                       "q": 2.0, "batch": {"insert": N_BATCH // 2, "delete": N_BATCH // 2},
+                       "form": "plain (one launch per job)"},
+            "walk_steps_per_s": r["walk_steps_per_s"], "edge_updates_per_s": r["edge_updates_per_s"],
+            "node2vec": {k: r[k] for k in ("trials_per_step", "probes_per_step")},
+            "roofline": {"bound": "hbm", "achieved": r["algorithmic_gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": r["algorithmic_gbs"] / peak, "traffic": None, "peak_source": peak_src,
+                         "kernel": "k_walk_plain<NODE2VEC>",
+                         "bytes": f"{N2V_BYTES_PER_TRIAL} B per proposal + {N2V_BYTES_PER_PROBE} B per probe"}}
+    print(json.dumps(line), flush=True)
 
 
 # --------------------------------------------------------------------------- GPU arm
@@ -831,9 +905,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"],
-                    help="plain: BASELINE config 2 (default); batched: config 4, batched vs plain; "
-                         "served: config 5, Poisson request stream, served vs plain")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "node2vec"],
+                    help="plain: BASELINE config 2 (default); node2vec: config 3; batched: config 4, batched vs "
+                         "plain; served: config 5, Poisson request stream, served vs plain")
     ap.add_argument("--served-scale", type=int, default=24)
     ap.add_argument("--rates", default="500,2000,8000", help="served: request rates (req/s) to sweep")
     ap.add_argument("--requests", type=int, default=400, help="served: requests per rate")
@@ -852,6 +926,8 @@ def main():
         run_batched(args)
     elif args.workload == "served" and args.impl == "ours":
         run_served(args)
+    elif args.workload == "node2vec" and args.impl == "ours":
+        run_node2vec(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-cuda":

@@ -114,6 +114,8 @@ class BingoStats(ctypes.Structure):
         ("scratch_bytes", c_uint64),
         ("walk_steps", c_uint64),
         ("kernel_launches", c_uint64),
+        ("walk_trials", c_uint64),
+        ("walk_probes", c_uint64),
     ]
 
 

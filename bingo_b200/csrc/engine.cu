@@ -279,6 +279,7 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP, MULTI))
   LaneWalk s;
   RowStage o{kNoSec, 0};
   uint32_t jid = 0, moves = 0, wb = 0, we = 0;
+  s.trials = 0, s.probes = 0;
   bool active = false, drained = false;
   for (;;) {
     uint32_t idle = __ballot_sync(kFull, !active);
@@ -331,6 +332,7 @@ __global__ void __launch_bounds__(kBlock, walk_min_blocks(APP, MULTI))
     }
   }
   add_steps(W, moves);
+  add_n2v(W, s);
 }
 
 __global__ void k_philox(const uint32_t* ctr, unsigned long long count, uint32_t k0, uint32_t k1, uint32_t* out) {
@@ -537,8 +539,8 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
   cuda_check(cudaMalloc(&d_err_, 4 * sizeof(uint32_t)), "cudaMalloc(err)");
   cuda_check(cudaMemset(d_err_, 0, 4 * sizeof(uint32_t)), "memset(err)");
   cuda_check(cudaMalloc(&d_top_, kArenas * sizeof(unsigned long long)), "cudaMalloc(top)");
-  cuda_check(cudaMalloc(&d_steps_, sizeof(unsigned long long)), "cudaMalloc(steps)");
-  cuda_check(cudaMemset(d_steps_, 0, sizeof(unsigned long long)), "memset(steps)");
+  cuda_check(cudaMalloc(&d_steps_, 3 * sizeof(unsigned long long)), "cudaMalloc(steps)");
+  cuda_check(cudaMemset(d_steps_, 0, 3 * sizeof(unsigned long long)), "memset(steps)");
   cuda_check(cudaMemset(d_top_, 0, kArenas * sizeof(unsigned long long)), "memset(top)");
   cuda_check(cudaMallocHost(&h_err_, 4 * sizeof(uint32_t)), "cudaMallocHost(err)");
   cuda_check(cudaMallocHost(&h_top_, kArenas * sizeof(unsigned long long)), "cudaMallocHost(top)");
@@ -604,6 +606,7 @@ WalkView Engine::wview() const {
   W.hash = arena_[A_HASH].as<HashEntry>();
   W.err = d_err_;
   W.steps = d_steps_;
+  W.n2v = d_steps_ + 1;
   return W;
 }
 
@@ -1635,12 +1638,18 @@ void Engine::stats(bingo_stats* out) {
   out->n = n_;
   out->weight_mode = cfg_.weight_mode;
   if (server_) {  // the scheduler owns the stream and the host mirrors
-    cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
+    unsigned long long c[3];
+    cuda_check(cudaMemcpy(c, d_steps_, sizeof c, cudaMemcpyDeviceToHost), "stats");
+    out->walk_steps = c[0], out->walk_trials = c[1], out->walk_probes = c[2];
     out->kernel_launches = launches_;
     return;
   }
   cuda_check(cudaStreamSynchronize(stream_), "stats");
-  cuda_check(cudaMemcpy(&out->walk_steps, d_steps_, 8, cudaMemcpyDeviceToHost), "stats");
+  {
+    unsigned long long c[3];
+    cuda_check(cudaMemcpy(c, d_steps_, sizeof c, cudaMemcpyDeviceToHost), "stats");
+    out->walk_steps = c[0], out->walk_trials = c[1], out->walk_probes = c[2];
+  }
   out->kernel_launches = launches_;
   if (!loaded_) return;
   read_tops();

@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(kServeBlock, 4)
   LaneWalk s;
   RowStage o{kNoSec, 0};
   uint32_t moves = 0, jseq = 0, nap = 256, poll_in = 0;
+  s.trials = 0, s.probes = 0;
   unsigned long long idle_ns = 0;
   uint32_t wj = 0, wb = 0, we = 0;  // this warp's claimed range: walks [wb, we) of job wj
   bool active = false;
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(kServeBlock, 4)
     }
   }
   add_steps(W, moves);
+  add_n2v(W, s);
 }
 
 uint64_t now_ns() {

@@ -51,6 +51,7 @@ struct WalkView {
   const HashEntry* __restrict__ hash;
   uint32_t* err;
   unsigned long long* steps;  // running count of produced steps (moves to a neighbour)
+  unsigned long long* n2v;    // node2vec: [0] proposals drawn, [1] adjacency probes
 };
 
 __device__ __forceinline__ VertexRec load_vrec(const WalkView& W, uint32_t u) {
@@ -151,6 +152,8 @@ struct LaneWalk {
   int32_t prev;    // previous vertex (node2vec), -1 before the first move
   uint32_t phoff;  // previous vertex's adjacency index (node2vec)
   uint32_t phmask;
+  uint32_t trials;  // node2vec proposals drawn by this lane (kept across its walks)
+  uint32_t probes;  // node2vec adjacency-index lookups by this lane
 };
 
 // Starts walk i; returns true if it still has steps to produce. Sampling jobs
@@ -214,6 +217,7 @@ __device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev
       unsigned long long region = 0;
       if (J.ret_excess > 0.0) {
         const unsigned long long wp = hash_weight(W.hash + R.hoff, R.hmask, (uint32_t)s.prev);
+        ++s.probes;
         if (wp) {
           const double T = (double)__ldg(&W.alias[R.aoff].T);
           const double D = __dmul_rn(J.ret_excess, (double)wp);
@@ -232,13 +236,16 @@ __device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev
           break;
         }
         x = sample_at(W, R, philox(s.i, s.j, 2 * t, J.job, J.k0, J.k1));
+        ++s.trials;
         bool ok;
-        if ((int32_t)x == s.prev)
+        if ((int32_t)x == s.prev) {
           ok = a.x < J.thr_ret;
-        else if (a.x < io_min)
+        } else if (a.x < io_min) {
           ok = true;
-        else
+        } else {
           ok = a.x < (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
+          ++s.probes;
+        }
         if (ok || t + 1 == kMaxNode2vecTrials) break;
       }
     } else {
@@ -283,6 +290,15 @@ __device__ __forceinline__ void add_steps(const WalkView& W, unsigned long long 
 #pragma unroll
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(kFull, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(W.steps, mine);
+}
+
+// The same for the node2vec proposal and probe counts (zero, and folded
+// away, in kernels without node2vec walks).
+__device__ __forceinline__ void add_n2v(const WalkView& W, const LaneWalk& s) {
+  unsigned long long t = s.trials, p = s.probes;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(kFull, t, o), p += __shfl_xor_sync(kFull, p, o);
+  if ((threadIdx.x & 31) == 0 && (t | p)) atomicAdd(W.n2v, t), atomicAdd(W.n2v + 1, p);
 }
 
 }  // namespace bingo

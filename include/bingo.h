@@ -108,6 +108,8 @@ typedef struct bingo_stats {
   uint64_t walk_steps;    /* walk steps produced since bingo_create (moves to a neighbour) */
   uint64_t kernel_launches; /* engine kernels launched since bingo_create (library sort/scan/select
                                kernels not included) */
+  uint64_t walk_trials;   /* node2vec proposals drawn since bingo_create (one alias draw each) */
+  uint64_t walk_probes;   /* node2vec adjacency-index lookups since bingo_create */
 } bingo_stats;
 
 /* Defaults for bingo_config (device 0, node2vec on, synchronous, factor 2). */
