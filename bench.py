@@ -345,7 +345,7 @@ def run_batched(args):
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
                 "data": "synthetic",
-                "config": {"workload": "batched-rmat22", "scale": B_SCALE, "m": int(len(src)),
+                "config": {"workload": f"batched-rmat{B_SCALE}", "scale": B_SCALE, "m": int(len(src)),
                            "weights": "uniform[1,65535]", "jobs": len(jobs), "phases": B_PHASES,
                            "walks_per_step": int(sum(len(j["starts"]) for j in jobs)),
                            "update_edges_per_step": int(sum(chunk)),
@@ -592,7 +592,7 @@ def run_reference_cuda(args):
     if n2v:
         from bingo_b200 import NODE2VEC
         ours = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=WALK_LEN, p=0.5, q=2.0)
-        cfg = {"workload": "plain-node2vec-rmat22-w16", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
+        cfg = {"workload": f"plain-node2vec-rmat{N_SCALE}-w16", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
                "weights": "zipf(1.2)[1,2^16)", "walks": n, "walk_len": WALK_LEN, "p": 0.5, "q": 2.0,
                "batch": {"insert": N_BATCH // 2, "delete": N_BATCH // 2},
                "note": "walk length 80 = the reference's compile-time LEN (include/api.h:12); its node2vec tests "
@@ -702,7 +702,7 @@ def run_node2vec(args):
     line = {"metric": "walk_steps_per_s", "value": r["value"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": (r["walk_kernel_ms_per_step"] + r["update_ms_per_step"]),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "plain-node2vec-rmat22", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
+            "config": {"workload": f"plain-node2vec-rmat{N_SCALE}", "scale": N_SCALE, "edge_factor": EDGE_FACTOR,
                        "m": int(len(src)), "weights": "zipf(1.2)[1,2^24)", "walks": n, "walk_len": N_LEN, "p": 0.5,
                        "q": 2.0, "batch": {"insert": N_BATCH // 2, "delete": N_BATCH // 2},
                        "form": "plain (one launch per job)"},
@@ -909,6 +909,8 @@ def main():
                     help="plain: BASELINE config 2 (default); node2vec: config 3; batched: config 4, batched vs "
                          "plain; served: config 5, Poisson request stream, served vs plain")
     ap.add_argument("--served-scale", type=int, default=24)
+    ap.add_argument("--scale", type=int, default=22,
+                    help="node2vec / batched: R-MAT scale (22 = the configs; smaller for profiler captures)")
     ap.add_argument("--rates", default="500,2000,8000", help="served: request rates (req/s) to sweep")
     ap.add_argument("--requests", type=int, default=400, help="served: requests per rate")
     ap.add_argument("--p-update", type=float, default=0.05, help="served: fraction of update requests")
@@ -920,6 +922,8 @@ def main():
     ap.add_argument("--gather-ceiling", action="store_true",
                     help="also measure the GPU's random 32-byte-sector read ceiling")
     args = ap.parse_args()
+    global N_SCALE, B_SCALE
+    N_SCALE = B_SCALE = args.scale
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.workload == "batched" and args.impl == "ours":

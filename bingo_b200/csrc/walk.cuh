@@ -144,6 +144,10 @@ __device__ __forceinline__ void stage_pad(RowStage& o, int32_t* out, int32_t (*o
   for (; g < g_end; ++g) __stcs(out + g, -1);
 }
 
+// node2vec trials a lane runs before it yields the rest of the step to the
+// next call (the rest of its warp moves on meanwhile).
+constexpr uint32_t kNode2vecTrialsPerCall = 3;
+
 struct LaneWalk {
   uint32_t i;      // walk index within its job
   uint32_t j;      // step being produced
@@ -154,6 +158,8 @@ struct LaneWalk {
   uint32_t phmask;
   uint32_t trials;  // node2vec proposals drawn by this lane (kept across its walks)
   uint32_t probes;  // node2vec adjacency-index lookups by this lane
+  uint32_t t;       // node2vec: trial of the step in progress (0 = a new step)
+  unsigned long long region;  // node2vec: return-region threshold of the step in progress
 };
 
 // Starts walk i; returns true if it still has steps to produce. Sampling jobs
@@ -188,6 +194,7 @@ __device__ __forceinline__ bool walk_begin(const WalkView& W, const WalkJobDev& 
   s.cur = start;
   s.pos = 0;
   s.prev = -1;
+  s.t = 0;
   const bool tail = APP == APP_PPR && (J.flags & kWalkPprTail);
   if (L > 1 || tail) return true;
   stage_flush(o, J.out, obuf);
@@ -211,43 +218,58 @@ __device__ __forceinline__ bool walk_advance(const WalkView& W, const WalkJobDev
   } else {
     uint32_t x;
     if (APP == APP_NODE2VEC && s.prev >= 0) {
-      // Return region: when 1/p exceeds the envelope max(1, 1/q), the excess
-      // mass (ret_excess x w(cur -> prev)) returns to prev directly, with
-      // probability D / (T + D) per trial (word y of the acceptance block).
-      unsigned long long region = 0;
-      if (J.ret_excess > 0.0) {
-        const unsigned long long wp = hash_weight(W.hash + R.hoff, R.hmask, (uint32_t)s.prev);
-        ++s.probes;
-        if (wp) {
-          const double T = (double)__ldg(&W.alias[R.aoff].T);
-          const double D = __dmul_rn(J.ret_excess, (double)wp);
-          region = prob_threshold_dev(__ddiv_rn(D, __dadd_rn(T, D)));
+      // One trial per call: a rejected lane keeps its step and retries on the
+      // next call while the other lanes of its warp go on, so the lanes of a
+      // warp stay on the same instruction path (the trial count per step
+      // varies from lane to lane). Trial t reads the same Philox blocks as in
+      // a loop, so the walk is unchanged.
+      if (s.t == 0) {
+        // Return region: when 1/p exceeds the envelope max(1, 1/q), the
+        // excess mass (ret_excess x w(cur -> prev)) returns to prev directly,
+        // with probability D / (T + D) per trial (word y of the acceptance
+        // block).
+        s.region = 0;
+        if (J.ret_excess > 0.0) {
+          const unsigned long long wp = hash_weight(W.hash + R.hoff, R.hmask, (uint32_t)s.prev);
+          ++s.probes;
+          if (wp) {
+            const double T = (double)__ldg(&W.alias[R.aoff].T);
+            const double D = __dmul_rn(J.ret_excess, (double)wp);
+            s.region = prob_threshold_dev(__ddiv_rn(D, __dadd_rn(T, D)));
+          }
         }
       }
       // Otherwise accept a proposal x with probability weight(class(x)) /
       // envelope. The adjacency probe is skipped when the acceptance draw is
       // below both the in- and out-class thresholds (the outcome is then the
       // same for every class x can be in).
-      const unsigned long long io_min = J.thr_in < J.thr_out ? J.thr_in : J.thr_out;
-      for (uint32_t t = 0;; ++t) {
-        const Rand4 a = philox(s.i, s.j, 2 * t + 1, J.job, J.k0, J.k1);
-        if ((unsigned long long)a.y < region) {
+      bool ok = false;
+      for (uint32_t k = 0; k < kNode2vecTrialsPerCall && !ok; ++k) {
+        if (k) ++s.t;
+        const Rand4 a = philox(s.i, s.j, 2 * s.t + 1, J.job, J.k0, J.k1);
+        if ((unsigned long long)a.y < s.region) {
           x = (uint32_t)s.prev;
-          break;
-        }
-        x = sample_at(W, R, philox(s.i, s.j, 2 * t, J.job, J.k0, J.k1));
-        ++s.trials;
-        bool ok;
-        if ((int32_t)x == s.prev) {
-          ok = a.x < J.thr_ret;
-        } else if (a.x < io_min) {
           ok = true;
         } else {
-          ok = a.x < (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
-          ++s.probes;
+          x = sample_at(W, R, philox(s.i, s.j, 2 * s.t, J.job, J.k0, J.k1));
+          ++s.trials;
+          const unsigned long long io_min = J.thr_in < J.thr_out ? J.thr_in : J.thr_out;
+          if ((int32_t)x == s.prev) {
+            ok = a.x < J.thr_ret;
+          } else if (a.x < io_min) {
+            ok = true;
+          } else {
+            ok = a.x < (hash_has(W.hash + s.phoff, s.phmask, x) ? J.thr_in : J.thr_out);
+            ++s.probes;
+          }
+          ok = ok || s.t + 1 == kMaxNode2vecTrials;
         }
-        if (ok || t + 1 == kMaxNode2vecTrials) break;
       }
+      if (!ok) {
+        ++s.t;
+        return true;  // the step continues on the next call
+      }
+      s.t = 0;
     } else {
       x = sample_at(W, R, philox(s.i, s.j, 0, J.job, J.k0, J.k1));
     }
