@@ -38,6 +38,7 @@ namespace {
 
 constexpr int kServeBlock = 256;
 constexpr uint32_t kPollSteps = 8;
+constexpr uint32_t kSpinPasses = 20000;  // scheduler passes polled without sleeping
 
 // Lane 0 of a warp: take up to 32 walks of the oldest job that has any left.
 // Returns the count taken (0: none now); *none_left is set when every
@@ -583,6 +584,7 @@ bool Server::step() {
 
 void Server::loop() {
   cudaSetDevice(eng_.device());
+  uint32_t quiet = 0;  // passes in a row without progress while work is in flight
   for (;;) {
     bool progress = false;
     try {
@@ -606,13 +608,20 @@ void Server::loop() {
     std::unique_lock<std::mutex> lk(mu_);
     const bool idle = queue_.empty() && inflight_.empty();
     if (quit_ && idle) break;
-    if (!progress) {
-      if (idle)
-        cv_.wait_for(lk, std::chrono::milliseconds(5));
-      else {
-        lk.unlock();
+    if (progress) {
+      quiet = 0;
+    } else if (idle) {
+      quiet = 0;
+      cv_.wait_for(lk, std::chrono::milliseconds(5));
+    } else {
+      // Work in flight: poll without sleeping for a while (a timed sleep
+      // costs tens of microseconds of timer slack on every hop of a
+      // request), then back off to short sleeps.
+      lk.unlock();
+      if (++quiet < kSpinPasses)
+        std::this_thread::yield();
+      else
         std::this_thread::sleep_for(std::chrono::microseconds(10));
-      }
     }
   }
   ctl_.stop = 1;
