@@ -62,12 +62,15 @@ __device__ __forceinline__ VertexRec load_vrec(const WalkView& W, uint32_t u) {
 // Weighted neighbour draw at a vertex with R.m > 0: slot = mulhi(x, m),
 // r = mulhi64(y:z, T), group = r < thr ? own : alias, member = mulhi(w, cnt).
 __device__ __forceinline__ uint32_t sample_at(const WalkView& W, const VertexRec& R, const Rand4& r) {
-  const ulonglong2* a = reinterpret_cast<const ulonglong2*>(W.alias + R.aoff + mulhi32(r.x, R.m));
-  const ulonglong2 tt = __ldg(a);                                   // thr, T
-  const uint4 g = __ldg(reinterpret_cast<const uint4*>(a + 1));     // own base/cnt, alt base/cnt
-  const unsigned long long d = mulhi64(((unsigned long long)r.y << 32) | r.z, tt.y);
-  const bool own = d < tt.x;
-  const uint32_t base = own ? g.x : g.z, cnt = own ? g.y : g.w;
+  // The whole 32-byte slot in one 256-bit read-only load (one L1 / L2
+  // request instead of two 16-byte ones; slots are 32-byte aligned and no
+  // kernel writes the store while walks run).
+  const AliasRec* a = W.alias + R.aoff + mulhi32(r.x, R.m);
+  unsigned long long thr, T, own_bc, alt_bc;
+  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(thr), "=l"(T), "=l"(own_bc), "=l"(alt_bc) : "l"(a));
+  const unsigned long long d = mulhi64(((unsigned long long)r.y << 32) | r.z, T);
+  const unsigned long long bc = d < thr ? own_bc : alt_bc;  // base | cnt << 32
+  const uint32_t base = (uint32_t)bc, cnt = (uint32_t)(bc >> 32);
   return __ldg(W.gv + (size_t)base * 4 + mulhi32(r.w, cnt));
 }
 
