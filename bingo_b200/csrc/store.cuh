@@ -21,24 +21,46 @@ __device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uin
   const uint32_t m = __popc(nz);
   if (m == 0) return 0;
   const unsigned long long T = warp_sum_u64(mass);
-  unsigned __int128 s = (unsigned __int128)mass * m;
-  uint32_t small = __ballot_sync(kFull, cnt != 0 && s < T);
-  uint32_t large = nz & ~small;
   unsigned long long thr = T;
   int alias_lane = lane;
-  while (small && large) {
-    const int a = __ffs(small) - 1, b = __ffs(large) - 1;
-    const unsigned long long sa = __shfl_sync(kFull, (unsigned long long)s, a);  // s_a < T fits 64 bits
-    if (lane == a) {
-      thr = sa;
-      alias_lane = b;
+  if (T < (1ull << 58)) {
+    // Every scaled mass is below 32 * 2^58: the same pairing in 64 bits.
+    unsigned long long s = mass * m;
+    uint32_t small = __ballot_sync(kFull, cnt != 0 && s < T);
+    uint32_t large = nz & ~small;
+    while (small && large) {
+      const int a = __ffs(small) - 1, b = __ffs(large) - 1;
+      const unsigned long long sa = __shfl_sync(kFull, s, a);
+      if (lane == a) {
+        thr = sa;
+        alias_lane = b;
+      }
+      if (lane == b) s -= T - sa;
+      small &= ~(1u << a);
+      const bool b_small = __shfl_sync(kFull, (int)(s < T), b);
+      if (b_small) {
+        large &= ~(1u << b);
+        small |= 1u << b;
+      }
     }
-    if (lane == b) s -= (unsigned __int128)(T - sa);
-    small &= ~(1u << a);
-    const bool b_small = __shfl_sync(kFull, (int)(s < T), b);
-    if (b_small) {
-      large &= ~(1u << b);
-      small |= 1u << b;
+  } else {
+    unsigned __int128 s = (unsigned __int128)mass * m;
+    uint32_t small = __ballot_sync(kFull, cnt != 0 && s < T);
+    uint32_t large = nz & ~small;
+    while (small && large) {
+      const int a = __ffs(small) - 1, b = __ffs(large) - 1;
+      const unsigned long long sa = __shfl_sync(kFull, (unsigned long long)s, a);  // s_a < T fits 64 bits
+      if (lane == a) {
+        thr = sa;
+        alias_lane = b;
+      }
+      if (lane == b) s -= (unsigned __int128)(T - sa);
+      small &= ~(1u << a);
+      const bool b_small = __shfl_sync(kFull, (int)(s < T), b);
+      if (b_small) {
+        large &= ~(1u << b);
+        small |= 1u << b;
+      }
     }
   }
   // Remaining groups hold exactly T: thr = T, alias = self (already set).
@@ -150,6 +172,12 @@ __device__ __forceinline__ GrowPlan plan_growth(int lane, const VertexMeta& M, c
 // total popcount, from one ballot per bit per 32 edges.
 __device__ __forceinline__ void count_bits(int lane, const uint32_t* seg_w, uint32_t len, uint32_t* add_lane,
                                            uint32_t* pc_total) {
+  if (len == 1) {  // one edge (the common case): lane k counts bit k of its weight
+    const uint32_t w = seg_w[0];
+    *add_lane = (w >> lane) & 1u;
+    *pc_total = __popc(w);
+    return;
+  }
   uint32_t add = 0, pc = 0;
   for (uint32_t c = 0; c < len; c += 32) {
     const uint32_t i = c + lane;
@@ -229,7 +257,25 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
 
   // --- append in batch order ---
   uint32_t bpbase = M.bpcnt;
-  for (uint32_t c = 0; c < len; c += 32) {
+  if (len == 1) {
+    // One edge: lane k appends it to group k at position cnt_k when its
+    // weight has bit k (the same positions the general loop gives).
+    const uint32_t v = seg_v[0], w = seg_w[0], slot = M.ecnt;
+    if (lane == 0) {
+      S.edges[M.eoff + slot] = EdgeRec{v, w, bpbase, 0u};
+      if (out_slots) out_slots[seg_orig[0]] = slot;
+    }
+    if ((w >> lane) & 1u) {
+      const uint32_t pos = G.cnt;
+      const size_t e = (size_t)G.base * 4 + pos;
+      S.gv[e] = v;
+      S.gs[e] = slot;
+      S.bp[M.bpoff + bpbase + __popc(w & ((1u << lane) - 1u))] = pos;
+      ++G.cnt;
+    }
+    bpbase += __popc(w);
+  }
+  for (uint32_t c = 0; len > 1 && c < len; c += 32) {
     const uint32_t i = c + lane;
     const bool valid = i < len;
     const uint32_t v = valid ? seg_v[i] : 0u, w = valid ? seg_w[i] : 0u;
