@@ -217,7 +217,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# --------------------------------------------------------------------------- batched (config 4)
+# --------------------------------------------------------------------------- batched: 256 mixed jobs on R-MAT 22
 B_SCALE, B_PHASES, B_JOBS_PER_PHASE = 22, 16, 16
 B_SEED = 1234 + 4
 
@@ -356,7 +356,7 @@ def run_batched(args):
         print(json.dumps(line), flush=True)
 
 
-# --------------------------------------------------------------------------- served (config 5)
+# --------------------------------------------------------------------------- served: Poisson requests on R-MAT 24
 S_SEED = 1234 + 5
 
 
@@ -555,7 +555,7 @@ def run_reference_cuda(args):
     total = args.warmup + args.steps
     w_hi = 1 << 16
     n2v = args.workload == "node2vec"
-    if n2v:  # config 3 with the reference's limits: weights < 2^16 (MAXLOG), its fixed LEN = 80, p = 0.5, q = 2
+    if n2v:  # node2vec on R-MAT 22 within the reference's limits: weights < 2^16 (MAXLOG), its fixed LEN = 80
         n, src, dst, w, batches = make_node2vec_workload(total, w_hi=w_hi - 1)
     else:
         n, src, dst, w, batches = make_workload(total, w_hi=w_hi)
@@ -667,7 +667,7 @@ def measure_engine(args, n, src, dst, w, batches, local, app=None, length=WALK_L
     return r
 
 
-# --------------------------------------------------------------------------- node2vec (config 3)
+# --------------------------------------------------------------------------- node2vec on R-MAT 22
 N_SCALE, N_LEN, N_BATCH = 22, 40, 1_000_000
 N_SEED = 1234 + 3
 N2V_BYTES_PER_TRIAL, N2V_BYTES_PER_PROBE = 32, 8  # algorithmic bytes: one alias draw; one adjacency lookup
@@ -688,7 +688,7 @@ def make_node2vec_workload(steps_total: int, w_hi: int = (1 << 24) - 1):
 
 
 def run_node2vec(args):
-    """Config 3 in the plain per-job form: node2vec (p = 0.5, q = 2) walks of
+    """node2vec in the plain per-job form: node2vec (p = 0.5, q = 2) walks of
     length 40 from every vertex of an R-MAT scale 22 graph with Zipf weights,
     after each 1M-edge update batch; device-timed, inputs in HBM."""
     from bingo_b200 import NODE2VEC
@@ -913,8 +913,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "node2vec"],
-                    help="plain: BASELINE config 2 (default); node2vec: config 3; batched: config 4, batched vs "
-                         "plain; served: config 5, Poisson request stream, served vs plain")
+                    help="plain: DeepWalk on R-MAT 20 with 50K+50K update batches (default); node2vec: node2vec on "
+                         "R-MAT 22 with 1M-edge batches; batched: 256 mixed jobs on R-MAT 22, batched vs plain; "
+                         "served: Poisson requests on R-MAT 24, served vs plain")
     ap.add_argument("--served-scale", type=int, default=24)
     ap.add_argument("--scale", type=int, default=22,
                     help="node2vec / batched: R-MAT scale (22 = the configs; smaller for profiler captures)")

@@ -74,9 +74,6 @@ __device__ __forceinline__ uint32_t sample_at(const WalkView& W, const VertexRec
   return __ldg(W.gv + (size_t)base * 4 + mulhi32(r.w, cnt));
 }
 
-__device__ __forceinline__ bool adjacent(const WalkView& W, const VertexRec& Rprev, uint32_t x) {
-  return hash_has(W.hash + Rprev.hoff, Rprev.hmask, x);
-}
 
 // ---------------------------------------------------------------------------
 // Step-at-a-time walks for the persistent kernels: a lane advances its walk

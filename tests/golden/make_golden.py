@@ -11,7 +11,7 @@ after every update batch:
 
 Each case becomes ref_<name>.npz (inputs + every dump). The config-1 sized
 case is too large to store whole, so only SHA-256 digests of its dumps are
-kept (ref_config1_digest.json); the test replays it on the CPU oracle.
+kept (ref_rmat14_digest.json); the test replays it on the CPU oracle.
 """
 from __future__ import annotations
 
@@ -82,13 +82,13 @@ CASES = {
     "edge": edge_case,
 }
 
-# BASELINE config 1 shape: R-MAT scale 14, edge factor 16, uniform [1,1024],
+# The small DeepWalk workload: R-MAT scale 14, edge factor 16, uniform [1,1024],
 # one batch of 10K absent-pair inserts and 10K uniform deletes.
-CONFIG1 = dict(scale=14, ef=16, seed=1234 + 1, lo=1, hi=1024, k=10000)
+RMAT14 = dict(scale=14, ef=16, seed=1234 + 1, lo=1, hi=1024, k=10000)
 
 
-def config1_case():
-    c = CONFIG1
+def rmat14_case():
+    c = RMAT14
     return rmat_case(c["scale"], c["ef"], c["seed"], gen.W_UNIFORM, c["lo"], c["hi"], 1, c["k"], c["k"])
 
 
@@ -143,14 +143,14 @@ def main():
         meta = dict(n=case["n"], rate=case["rate"], ops=kinds, source="oracle/_ref/ref_harness")
         np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"), meta=json.dumps(meta), **arrays)
         print(name, "ok", len(dumps), "dumps")
-    case = config1_case()
-    dumps, log = run_harness(case, args.out, "config1")
-    rec = dict(config=CONFIG1, inputs={k: digest(case[k]) for k in ("src", "dst", "w")},
+    case = rmat14_case()
+    dumps, log = run_harness(case, args.out, "rmat14")
+    rec = dict(config=RMAT14, inputs={k: digest(case[k]) for k in ("src", "dst", "w")},
                ops=[{"kind": op[0], "cols": [digest(c) for c in op[1:]]} for op in case["ops"]],
                dumps=[{k: digest(d[k]) for k in po.REF_DUMP_FIELDS} for d in dumps], harness_log=log)
-    with open(os.path.join(args.out, "ref_config1_digest.json"), "w") as f:
+    with open(os.path.join(args.out, "ref_rmat14_digest.json"), "w") as f:
         json.dump(rec, f, indent=1)
-    print("config1 ok")
+    print("rmat14 ok")
 
 
 if __name__ == "__main__":

@@ -40,8 +40,8 @@ def test_state_parity_small(dist, lo, hi):
     replay(n, src, dst, w, ops)
 
 
-def test_state_parity_config1():
-    """BASELINE config 1 shape: R-MAT 14 / ef 16, uniform [1,1024], 10K + 10K."""
+def test_state_parity_rmat14():
+    """The small DeepWalk workload: R-MAT 14 / ef 16, uniform [1,1024], 10K + 10K."""
     n, src, dst, w, ops = workload(scale=14, ef=16, seed=1235, rounds=1, k_ins=10000, k_del=10000)
     replay(n, src, dst, w, ops)
 
@@ -78,7 +78,7 @@ def _walk_both(g, ex, n, app, L, starts, mode, **kw):
 
 
 @pytest.fixture(scope="module")
-def config1_graphs():
+def rmat14_graphs():
     n, src, dst, w, ops = workload(scale=14, ef=16, seed=1235, rounds=1, k_ins=10000, k_del=10000)
     g = Graph()
     ex = po.ExactGraph(n)
@@ -91,8 +91,8 @@ def config1_graphs():
 @pytest.mark.parametrize("app,kw", [(DEEPWALK, {}), (NODE2VEC, dict(p=0.5, q=2.0)), (NODE2VEC, dict(p=4.0, q=0.25)),
                                     (PPR, dict(stop_prob=0.15)), (PPR, dict(stop_prob=0.0125, flags=WALK_PPR_TAIL)),
                                     (SAMPLING, {})])
-def test_walk_parity(config1_graphs, app, kw, mode):
-    n, g, ex, _ = config1_graphs
+def test_walk_parity(rmat14_graphs, app, kw, mode):
+    n, g, ex, _ = rmat14_graphs
     starts = np.arange(n, dtype=np.uint32)
     out, ref = _walk_both(g, ex, n, app, 80, starts, mode, seed=0xB1460 + app, job_id=3, **kw)
     assert np.array_equal(out, ref)
@@ -107,8 +107,8 @@ def test_walk_parity_after_updates():
         assert np.array_equal(out, ref), app
 
 
-def test_batched_heterogeneous_jobs(config1_graphs):
-    n, g, ex, _ = config1_graphs
+def test_batched_heterogeneous_jobs(rmat14_graphs):
+    n, g, ex, _ = rmat14_graphs
     rng = np.random.default_rng(0)
     jobs, refs = [], []
     specs = [(DEEPWALK, 10, {}), (NODE2VEC, 37, dict(p=0.25, q=4.0)), (PPR, 200, dict(stop_prob=0.15)),
@@ -130,8 +130,8 @@ def test_batched_heterogeneous_jobs(config1_graphs):
         assert np.array_equal(j.out, r)
 
 
-def test_walk_range_and_empty(config1_graphs):
-    n, g, ex, _ = config1_graphs
+def test_walk_range_and_empty(rmat14_graphs):
+    n, g, ex, _ = rmat14_graphs
     out = g.walk(app=DEEPWALK, length=80, first=100, n_starts=500, seed=5)
     ref = ex.walk(DEEPWALK, 80, np.arange(100, 600, dtype=np.uint32), seed=5)
     assert np.array_equal(out, ref)
@@ -141,9 +141,9 @@ def test_walk_range_and_empty(config1_graphs):
     assert np.array_equal(one[:, 0], np.arange(10))
 
 
-def test_device_tensors(config1_graphs):
+def test_device_tensors(rmat14_graphs):
     torch = pytest.importorskip("torch")
-    n, g, ex, _ = config1_graphs
+    n, g, ex, _ = rmat14_graphs
     starts = torch.arange(0, n, dtype=torch.int32, device="cuda")
     out = torch.empty((n, 40), dtype=torch.int32, device="cuda")
     g.walk(app=DEEPWALK, length=40, starts=starts, out=out, seed=12)

@@ -172,17 +172,17 @@ def test_reference_literal_matches_reference_dumps(path):
         compare_exact_vs_ref(ex.dump(), mine, n)
 
 
-def test_reference_config1_digests():
-    """BASELINE config 1 shape (R-MAT 14, uniform [1,1024], 10K + 10K): the
+def test_reference_rmat14_digests():
+    """The small DeepWalk workload (R-MAT 14, uniform [1,1024], 10K + 10K): the
     reference binary's dumps after load, insert and delete, stored as SHA-256
     digests, equal the reference-literal oracle replaying the same inputs."""
     import hashlib
     import importlib.util
-    rec = json.load(open(os.path.join(GOLDEN, "ref_config1_digest.json")))
+    rec = json.load(open(os.path.join(GOLDEN, "ref_rmat14_digest.json")))
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
     mg = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mg)
-    case = mg.config1_case()
+    case = mg.rmat14_case()
     dig = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
     for k in ("src", "dst", "w"):
         assert dig(case[k]) == rec["inputs"][k], f"input {k} drifted from the fixture"
@@ -195,7 +195,7 @@ def test_reference_config1_digests():
     assert len(dumps) == len(rec["dumps"])
     for i, (mine, want) in enumerate(zip(dumps, rec["dumps"])):
         for k in po.REF_DUMP_FIELDS:
-            assert dig(mine[k]) == want[k], f"config1 dump {i} field {k}"
+            assert dig(mine[k]) == want[k], f"rmat14 dump {i} field {k}"
 
 
 def test_oracle_delete_pairs_rank_semantics():
