@@ -42,6 +42,12 @@ int sm_count() {
   return sms;
 }
 
+size_t pow2_bytes(size_t b) {
+  size_t p = 256;
+  while (p < b) p <<= 1;
+  return p;
+}
+
 unsigned grid_for(unsigned long long items, unsigned per_block, unsigned max_per_sm = 8) {
   const unsigned long long want = (items + per_block - 1) / per_block;
   const unsigned long long cap = (unsigned long long)sm_count() * max_per_sm;
@@ -1124,7 +1130,10 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
     }
     prefix[j + 1] = prefix[j] + J.n_starts;
   }
-  if (s_total) wstart_.ensure(s_total * 4, "walk staging");
+  // Staging grows to the next power of two, so a stream of queries of
+  // varying size reallocates (a device-wide synchronising cudaFree plus a
+  // cudaMalloc) only a few times.
+  if (s_total) wstart_.ensure(pow2_bytes(s_total * 4), "walk staging");
   // Host-bound outputs go through the next staging buffer; its previous
   // copy-out must finish before these kernels overwrite it (a device-side
   // wait, no host synchronisation).
@@ -1133,12 +1142,12 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   if (o_total) {
     wout_next_ ^= 1;
     if (wout_busy_[ring]) {
-      if (wout_[ring].bytes < o_total * 4)  // about to reallocate: its copy-out must be over first
+      if (wout_[ring].bytes < pow2_bytes(o_total * 4))  // about to reallocate: its copy-out must be over first
         cuda_check(cudaEventSynchronize(copy_ev_[ring]), "staging reuse");
       else
         cuda_check(cudaStreamWaitEvent(stream_, copy_ev_[ring], 0), "staging reuse");
     }
-    wout_[ring].ensure(o_total * 4, "walk staging");
+    wout_[ring].ensure(pow2_bytes(o_total * 4), "walk staging");
     wout = wout_[ring].as<int32_t>();
   }
   for (uint32_t j = 0; j < n_jobs; ++j) {

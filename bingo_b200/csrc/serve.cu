@@ -112,7 +112,9 @@ __global__ void __launch_bounds__(kServeBlock, 4)
       if (wb >= we) {
         if (!may_claim) break;
         uint32_t cj = 0, cb = 0, got = 0;
-        if (lane == 0) {
+        // A closing kernel takes no new walks (its warps finish the walks
+        // they hold and exit; the host relaunches a full grid for the rest).
+        if (lane == 0 && !reinterpret_cast<volatile ServeDevState*>(st)->closing) {
           bool nl = false;
           got = claim_walks(jobs, ctl, st, err_word, &cj, &cb, &nl);
           none_left = nl;
