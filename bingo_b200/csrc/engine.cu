@@ -566,7 +566,8 @@ Engine::~Engine() {
   prog_jobs_.release(), prog_prefix_.release(), prog_queue_.release();
   DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
                     &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
-                    &prefix_, &queue_, &wstart_, &wout_[0], &wout_[1], &pair_key_, &pair_key_s_, &pair_slot_};
+                    &prefix_, &queue_, &wstart_, &wout_[0], &wout_[1], &pair_key_, &pair_key_s_, &pair_slot_,
+                    &fw_in_, &fw_fixed_};
   for (DevBuf* b : bufs) b->release();
   for (int k = 0; k < 2; ++k) {
     if (walk_ev_[k]) cudaEventDestroy(walk_ev_[k]);
@@ -1671,7 +1672,8 @@ void Engine::stats(bingo_stats* out) {
   }
   const DevBuf* sc[] = {&in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_, &sb_, &head_, &seg_, &nseg_,
                         &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_, &prefix_, &queue_, &wstart_,
-                        &wout_[0], &wout_[1]};
+                        &wout_[0], &wout_[1], &pair_key_, &pair_key_s_, &pair_slot_, &fw_in_, &fw_fixed_,
+                        &prog_jobs_, &prog_prefix_, &prog_queue_};
   for (const DevBuf* b : sc) out->scratch_bytes += b->bytes;
 }
 
