@@ -1060,17 +1060,31 @@ void Engine::erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k) {
   if (!is_device_ptr(u)) host_check_ids(u, k, n_, "vertex");
   if (!is_device_ptr(v)) host_check_ids(v, k, n_, "vertex");
   ensure_batch_scratch(k);
-  pair_key_.ensure(k * 8, "scratch");
-  pair_key_s_.ensure(k * 8, "scratch");
-  pair_slot_.ensure(k * 4, "scratch");
-  int end_bit = 33;
-  while (end_bit < 64 && (1ull << (end_bit - 32)) < n_) ++end_bit;
-  size_t t_sort = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                  (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)k, 0, end_bit, stream_);
-  cub_tmp_.ensure(t_sort, "scratch");
+  ensure_pair_scratch(k);
   const uint32_t* du = stage(u, k, in_a_, "stage u");
   const uint32_t* dv = stage(v, k, in_b_, "stage v");
+  translate_pairs(du, dv, k);
+  erase(du, pair_slot_.as<uint32_t>(), k);
+}
+
+// Scratch for translating k pairs (sized before a program is captured).
+void Engine::ensure_pair_scratch(uint64_t k) {
+  const uint64_t kk = std::max<uint64_t>(k, 1);
+  pair_key_.ensure(kk * 8, "scratch");
+  pair_key_s_.ensure(kk * 8, "scratch");
+  pair_slot_.ensure(kk * 4, "scratch");
+  size_t t_sort = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                  (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)kk, 0, 64, stream_);
+  cub_tmp_.ensure(t_sort, "scratch");
+}
+
+// Device arrays u, v -> pair_slot_ (stream-ordered, no host synchronisation):
+// stable sort of (u << 32 | v), runs of equal pairs, one warp per run
+// scanning u's slots. A batch that fails validation keeps every slot absent.
+void Engine::translate_pairs(const uint32_t* du, const uint32_t* dv, uint64_t k) {
+  int end_bit = 33;
+  while (end_bit < 64 && (1ull << (end_bit - 32)) < n_) ++end_bit;
   cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
   k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, dv, nullptr, k, n_, ctl_.as<uint32_t>(), d_err_);
   k_pair_keys<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, dv, k, pair_key_.as<unsigned long long>());
@@ -1097,7 +1111,6 @@ void Engine::erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k) {
       nseg_.as<uint32_t>(), k, ctl_.as<uint32_t>(), pair_slot_.as<uint32_t>());
   cuda_check(cudaGetLastError(), "pair slots");
   ++launches_;
-  erase(du, pair_slot_.as<uint32_t>(), k);
 }
 
 void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
@@ -1379,14 +1392,15 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
   if (!ops) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null op array");
   const bool use_graph = flags & BINGO_RUN_GRAPH;
   // ---- validate, size scratch, lay out the job tables
-  uint64_t kmax = 0, k_ins = 0, n_jobs_total = 0, n_walk_ops = 0;
+  uint64_t kmax = 0, k_ins = 0, n_jobs_total = 0, n_walk_ops = 0, kpairs = 0;
   uint64_t sig = 1469598103934665603ull;
   auto mix = [&](uint64_t x) { sig = (sig ^ x) * 1099511628211ull; };
   for (uint32_t i = 0; i < n_ops; ++i) {
     const bingo_op& o = ops[i];
     mix((uint64_t)o.kind);
-    if (o.kind == BINGO_OP_INSERT || o.kind == BINGO_OP_DELETE) {
+    if (o.kind == BINGO_OP_INSERT || o.kind == BINGO_OP_DELETE || o.kind == BINGO_OP_DELETE_PAIRS) {
       const bool ins = o.kind == BINGO_OP_INSERT;
+      if (o.kind == BINGO_OP_DELETE_PAIRS && o.k) kpairs = std::max<uint64_t>(kpairs, o.k);
       if (!o.k) continue;
       if (o.k >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "batch larger than 2^31");
       if (!o.a || !o.b || (ins && !o.c)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null batch array");
@@ -1408,6 +1422,7 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
     }
   }
   if (kmax) ensure_batch_scratch(kmax);
+  if (kpairs) ensure_pair_scratch(kpairs);
   ensure_headroom(k_ins);
   mix(arena_gen_), mix(n_);
   std::vector<WalkJobDev> dj, table;
@@ -1488,6 +1503,9 @@ void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
         enqueue_insert(o.a, o.b, o.c, o.k, o.out_slots);
       } else if (o.kind == BINGO_OP_DELETE && o.k) {
         enqueue_delete(o.a, o.b, o.k);
+      } else if (o.kind == BINGO_OP_DELETE_PAIRS && o.k) {
+        translate_pairs(o.a, o.b, o.k);
+        enqueue_delete(o.a, pair_slot_.as<uint32_t>(), o.k);
       } else if (o.kind == BINGO_OP_WALK) {
         for (size_t gi = grp_begin[i]; gi < grp_end[i]; ++gi) {
           const WalkGroup& G = groups[gi];

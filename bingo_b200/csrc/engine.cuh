@@ -171,6 +171,8 @@ class Engine {
   void insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots);
   void erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k);
   const uint32_t* fixed_weights(const float* w, uint64_t k);
+  void ensure_pair_scratch(uint64_t k);
+  void translate_pairs(const uint32_t* du, const uint32_t* dv, uint64_t k);
   void check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k);
   bool save_state(StateCopy& c);
   void restore_state(const StateCopy& c);

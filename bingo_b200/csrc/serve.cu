@@ -279,7 +279,8 @@ uint64_t Server::submit_walk(const bingo_walk_job& J) {
 
 uint64_t Server::submit_update(int kind, const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k,
                                uint32_t* out_slots) {
-  if (kind != BINGO_OP_INSERT && kind != BINGO_OP_DELETE) throw Error(BINGO_ERR_INVALID_ARGUMENT, "bad update kind");
+  if (kind != BINGO_OP_INSERT && kind != BINGO_OP_DELETE && kind != BINGO_OP_DELETE_PAIRS)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "bad update kind");
   if (k && (!a || !b || (kind == BINGO_OP_INSERT && !c))) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null batch array");
   Request r;
   r.kind = kind;
@@ -539,18 +540,23 @@ bool Server::step() {
       if (kernel_running()) break;
       const uint64_t t_upd = now_ns();
       int st = BINGO_OK;
-      try {
-        const uint64_t k = r->a.size();
-        for (uint64_t o = 0; o < k; o += cfg_.max_update_batch) {
-          const uint64_t len = std::min<uint64_t>(cfg_.max_update_batch, k - o);
+      const uint64_t k = r->a.size();
+      for (uint64_t o = 0; o < k; o += cfg_.max_update_batch) {
+        const uint64_t len = std::min<uint64_t>(cfg_.max_update_batch, k - o);
+        try {
           if (r->kind == BINGO_OP_INSERT)
             eng_.insert(r->a.data() + o, r->b.data() + o, r->c.data() + o, len,
                         r->out_slots ? r->out_slots + o : nullptr);
+          else if (r->kind == BINGO_OP_DELETE_PAIRS)  // chunks see earlier chunks' deletes: same slots
+            eng_.erase_pairs(r->a.data() + o, r->b.data() + o, len);
           else
             eng_.erase(r->a.data() + o, r->b.data() + o, len);
+        } catch (const Error& e) {
+          st = e.status;
+          // Skipped deletes are reported after the rest of the batch applies;
+          // any other error ends the batch.
+          if (st != BINGO_ERR_INVALID_SLOT) break;
         }
-      } catch (const Error& e) {
-        st = e.status;
       }
       ++version_;
       ctl_.drain = 0;

@@ -22,7 +22,7 @@ DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
 WALK_PPR_TAIL = 1
 BATCHED, PLAIN = 0, 1
-OP_WALK, OP_INSERT, OP_DELETE = 0, 1, 2
+OP_WALK, OP_INSERT, OP_DELETE, OP_DELETE_PAIRS = 0, 1, 2, 3
 RUN_GRAPH = 1
 
 
@@ -212,7 +212,7 @@ class Graph:
 
     def run(self, ops: Sequence[tuple], graph: bool = True):
         """Run a program: a list of ("walk", [WalkJob...]), ("insert", src, dst,
-        w[, out_slots]) and ("delete", u, slot) with device tensors, in order
+        w[, out_slots]), ("delete", u, slot) and ("delete_pairs", u, v) with device tensors, in order
         and without host synchronisation (bingo_run). graph=True captures it
         into a CUDA graph replayed while its shape is unchanged."""
         arr = (BingoOp * len(ops))()
@@ -224,10 +224,10 @@ class Graph:
                 keep.append(jobs)
                 arr[i].kind, arr[i].n_jobs = OP_WALK, len(op[1])
                 arr[i].jobs = ctypes.cast(jobs, ctypes.POINTER(BingoWalkJob))
-            elif kind in ("insert", "delete"):
+            elif kind in ("insert", "delete", "delete_pairs"):
                 cols = [_u32(x) for x in op[1:4 if kind == "insert" else 3]]
                 keep += [c[1] for c in cols]
-                arr[i].kind = OP_INSERT if kind == "insert" else OP_DELETE
+                arr[i].kind = {"insert": OP_INSERT, "delete": OP_DELETE, "delete_pairs": OP_DELETE_PAIRS}[kind]
                 arr[i].a, arr[i].b = cols[0][0], cols[1][0]
                 if kind == "insert":
                     arr[i].c = cols[2][0]
@@ -281,8 +281,12 @@ class Graph:
         return t.value, out
 
     def submit_update(self, kind: str, a, b, c=None, out_slots=None):
-        """Submit an insert (a = src, b = dst, c = weights) or delete (a = vertex,
-        b = slot) batch; returns (ticket, out_slots) (slots filled for inserts)."""
+        """Submit an insert (a = src, b = dst, c = weights), delete (a = vertex,
+        b = slot) or delete_pairs (a = u, b = v) batch; returns (ticket,
+        out_slots) (slots filled for inserts)."""
+        code = {"insert": OP_INSERT, "delete": OP_DELETE, "delete_pairs": OP_DELETE_PAIRS}.get(kind)
+        if code is None:
+            raise ValueError(f"unknown update kind {kind!r}")
         k = len(a) if not hasattr(a, "numel") else a.numel()
         pa, ka = _u32(a)
         pb, kb = _u32(b)
@@ -291,8 +295,7 @@ class Graph:
             out_slots = np.zeros(k, np.uint32)
         po = _out(out_slots, np.uint32)[0] if out_slots is not None else None
         t = ctypes.c_uint64()
-        self._check(self._L.bingo_serve_submit_update(self._h, OP_INSERT if kind == "insert" else OP_DELETE, pa, pb,
-                                                      pc, k, po, ctypes.byref(t)))
+        self._check(self._L.bingo_serve_submit_update(self._h, code, pa, pb, pc, k, po, ctypes.byref(t)))
         self._serve_keep[t.value] = out_slots
         return t.value, out_slots
 

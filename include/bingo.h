@@ -207,16 +207,21 @@ int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_j
  * replays. Update capacity is checked on the device: a batch that does not
  * fit the graph arenas is not applied and the call returns
  * BINGO_ERR_CAPACITY (the arenas are grown before the next call). */
-typedef enum bingo_op_kind { BINGO_OP_WALK = 0, BINGO_OP_INSERT = 1, BINGO_OP_DELETE = 2 } bingo_op_kind;
+typedef enum bingo_op_kind {
+  BINGO_OP_WALK = 0,
+  BINGO_OP_INSERT = 1,
+  BINGO_OP_DELETE = 2,
+  BINGO_OP_DELETE_PAIRS = 3 /* delete by (u, v) as bingo_delete_pairs */
+} bingo_op_kind;
 
 typedef struct bingo_op {
   int32_t kind;               /* bingo_op_kind */
   uint32_t n_jobs;            /* WALK: jobs in this set, run as one persistent launch */
   const bingo_walk_job* jobs; /* WALK */
-  const uint32_t* a;          /* INSERT: src   DELETE: vertex */
-  const uint32_t* b;          /* INSERT: dst   DELETE: slot */
+  const uint32_t* a;          /* INSERT: src   DELETE: vertex   DELETE_PAIRS: u */
+  const uint32_t* b;          /* INSERT: dst   DELETE: slot     DELETE_PAIRS: v */
   const uint32_t* c;          /* INSERT: weight */
-  uint64_t k;                 /* INSERT / DELETE: batch size */
+  uint64_t k;                 /* INSERT / DELETE / DELETE_PAIRS: batch size */
   uint32_t* out_slots;        /* INSERT: slot ids (device, may be NULL) */
 } bingo_op;
 
@@ -258,8 +263,9 @@ typedef struct bingo_serve_status {
 
 int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg);
 int bingo_serve_submit_walk(bingo_handle* h, const bingo_walk_job* job, uint64_t* ticket);
-/* kind: BINGO_OP_INSERT (a = src, b = dst, c = weights, out_slots optional)
- * or BINGO_OP_DELETE (a = vertex, b = slot). */
+/* kind: BINGO_OP_INSERT (a = src, b = dst, c = weights, out_slots optional),
+ * BINGO_OP_DELETE (a = vertex, b = slot) or BINGO_OP_DELETE_PAIRS (a = u,
+ * b = v, as bingo_delete_pairs). */
 int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, const uint32_t* b,
                               const uint32_t* c, uint64_t k, uint32_t* out_slots, uint64_t* ticket);
 int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);

@@ -80,3 +80,41 @@ def test_delete_pairs_out_of_range_rejects_batch():
     with pytest.raises(BingoError):
         g.delete_pairs(torch.from_numpy(u.view(np.int32)).cuda(), torch.from_numpy(v.view(np.int32)).cuda())
     assert_exact_equal(g.dump(), before)
+
+
+def test_delete_pairs_in_programs_and_serving():
+    """The same translation inside a captured program (replayed with new
+    contents) and as a served update: state equals the oracle's."""
+    import torch
+    n, src, dst, w, par = _graph_with_parallel_edges(10, 13)
+    rng = np.random.default_rng(4)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.uint32).view(np.int32)).cuda()  # noqa: E731
+    g, ex = Graph(node2vec=True), po.ExactGraph(n)
+    g.load_edges(src, dst, w, n)
+    ex.load(src, dst, w)
+    k = 3000
+    for rnd in range(2):  # second round replays the captured graph with new batch contents
+        i = rng.choice(len(src), size=k)
+        u = np.concatenate([src[i], par[0][:500]]).astype(np.uint32)
+        v = np.concatenate([dst[i], par[1][:500]]).astype(np.uint32)
+        if rnd == 0:
+            du, dv = dev(u), dev(v)
+        else:
+            du.copy_(dev(u))
+            dv.copy_(dev(v))
+        bad, _ = ex.delete_pairs(u, v)
+        if bad:  # repeats beyond a pair's live edges: skipped, reported after the rest applied
+            with pytest.raises(BingoError, match="absent"):
+                g.run([("delete_pairs", du, dv)], graph=True)
+        else:
+            g.run([("delete_pairs", du, dv)], graph=True)
+        assert_exact_equal(g.dump(), ex.dump(), f"program round {rnd}: ")
+    g.serve_start(output_budget_bytes=64 << 20, max_update_batch=1000)  # chunks see earlier chunks' deletes
+    i = rng.choice(len(src), size=k)
+    u, v = src[i].astype(np.uint32), dst[i].astype(np.uint32)
+    t, _ = g.submit_update("delete_pairs", u, v)
+    st = g.serve_wait(t)
+    g.serve_stop()
+    bad, _ = ex.delete_pairs(u, v)
+    assert st["done"] and (st["status"] == 0) == (bad == 0)
+    assert_exact_equal(g.dump(), ex.dump(), "served: ")
