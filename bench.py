@@ -165,7 +165,8 @@ class CpuRun:
         self.ex = po.ExactGraph(n)
         self.ex.load(src, dst, w)
 
-    def step(self, batch, walks: int, seed: int):
+    def step(self, batch, walks: int, seed: int, app: int = 0, length: int = WALK_LEN, p: float = 0.5,
+             q: float = 2.0):
         ins, dels = batch
         t0 = time.perf_counter()
         self.ex.insert(*ins)
@@ -174,7 +175,7 @@ class CpuRun:
         rng = np.random.default_rng(seed)
         starts = np.sort(rng.choice(self.n, size=walks, replace=False)).astype(np.uint32)
         t0 = time.perf_counter()
-        rows = self.ex.walk(0, WALK_LEN, starts, seed=seed, job_id=0)
+        rows = self.ex.walk(app, length, starts, seed=seed, job_id=0, p=p, q=q)
         t_walk = time.perf_counter() - t0
         steps = int((rows >= 0).sum() - len(starts))
         scale = self.n / walks  # extrapolate the walk sample to one walk per vertex
@@ -627,6 +628,14 @@ def run_node2vec(args):
     n, src, dst, w, batches = make_node2vec_workload(total)
     r = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=N_LEN, p=0.5, q=2.0)
     peak, peak_src = peak_hbm()
+    cpu = None
+    if not args.no_cpu:
+        walks = min(args.cpu_walks, n)
+        c = CpuRun(n, src, dst, w).step(batches[0], walks, seed=7, app=NODE2VEC, length=N_LEN, p=0.5, q=2.0)
+        cpu = {"value": c["value"], "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"one full 500K+500K update batch + {walks} node2vec walks x {N_LEN} on the CPU oracle "
+                         f"(OpenMP), walk time scaled to {n} walks",
+               "walk_steps_per_s": c["walk_steps_per_s"], "edge_updates_per_s": c["edge_updates_per_s"]}
     line = {"metric": "walk_steps_per_s", "value": r["value"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": (r["walk_kernel_ms_per_step"] + r["update_ms_per_step"]),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -639,7 +648,8 @@ def run_node2vec(args):
             "roofline": {"bound": "hbm", "achieved": r["algorithmic_gbs"], "peak": peak, "unit": "GB/s",
                          "frac": r["algorithmic_gbs"] / peak, "traffic": None, "peak_source": peak_src,
                          "kernel": "k_walk_plain<NODE2VEC>",
-                         "bytes": f"{N2V_BYTES_PER_TRIAL} B per proposal + {N2V_BYTES_PER_PROBE} B per probe"}}
+                         "bytes": f"{N2V_BYTES_PER_TRIAL} B per proposal + {N2V_BYTES_PER_PROBE} B per probe"},
+            "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
 
 
