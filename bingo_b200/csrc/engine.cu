@@ -845,6 +845,7 @@ void host_check_weights(const uint32_t* w, uint64_t k) {
 }  // namespace
 
 void Engine::load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t m, uint32_t n) {
+  const NvtxRange nvtx_("bingo load");
   if (n == 0) throw Error(BINGO_ERR_INVALID_ARGUMENT, "n must be > 0");
   if (m && (!src || !dst || !w)) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null edge array");
   if (m >= (1ull << 31)) throw Error(BINGO_ERR_UNSUPPORTED, "more than 2^31 edges in one load");
@@ -894,6 +895,7 @@ void Engine::load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, u
 }
 
 void Engine::insert(const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k, uint32_t* out_slots) {
+  const NvtxRange nvtx_("bingo insert");
   require_loaded();
   if (k == 0) return;
   if (!src || !dst || !w) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null edge array");
@@ -1011,6 +1013,7 @@ void Engine::insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t
 }
 
 void Engine::erase(const uint32_t* u, const uint32_t* slot, uint64_t k) {
+  const NvtxRange nvtx_("bingo delete");
   require_loaded();
   if (k == 0) return;
   if (!u || !slot) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null delete array");
@@ -1053,6 +1056,7 @@ void Engine::erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k) {
 // slots. The translated (u, slot) batch then takes the slot-delete path, so
 // the swap-remove order is the batch order.
 void Engine::erase_pairs(const uint32_t* u, const uint32_t* v, uint64_t k) {
+  const NvtxRange nvtx_("bingo delete pairs");
   require_loaded();
   if (k == 0) return;
   if (!u || !v) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null delete array");
@@ -1114,6 +1118,7 @@ void Engine::translate_pairs(const uint32_t* du, const uint32_t* dv, uint64_t k)
 }
 
 void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
+  const NvtxRange nvtx_("bingo walk");
   require_loaded();
   if (n_jobs == 0) return;
   if (!jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
@@ -1387,6 +1392,7 @@ void Engine::ensure_headroom(uint64_t k_ins) {
 }
 
 void Engine::run(const bingo_op* ops, uint32_t n_ops, uint32_t flags) {
+  const NvtxRange nvtx_("bingo run");
   require_loaded();
   if (n_ops == 0) return;
   if (!ops) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null op array");
@@ -1580,6 +1586,7 @@ NoAllocScratch* noalloc_scratch(int device) {
 }  // namespace
 
 void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
+  const NvtxRange nvtx_("bingo walk noalloc");
   require_loaded();
   if (n_jobs == 0) return;
   if (!jobs) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null job array");
@@ -1933,6 +1940,7 @@ struct File {
 }  // namespace
 
 void Engine::save(const char* path) {
+  const NvtxRange nvtx_("bingo save");
   require_loaded();
   require_idle();
   if (!path) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null path");
@@ -2005,6 +2013,7 @@ void Engine::save(const char* path) {
 }
 
 void Engine::restore(const char* path) {
+  const NvtxRange nvtx_("bingo restore");
   require_idle();
   if (!path) throw Error(BINGO_ERR_INVALID_ARGUMENT, "null path");
   File F(path, "rb");

@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/bingo.h"
 #include "common.cuh"
 #include "walk.cuh"
@@ -22,6 +24,15 @@ struct Error : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+
+// NVTX range over one public operation, for Nsight timelines (a no-op when
+// no tool is attached; the NVTX v3 header needs no library).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Device buffer that grows by reallocation (contents not preserved).
 struct DevBuf {

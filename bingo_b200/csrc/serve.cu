@@ -539,6 +539,7 @@ bool Server::step() {
       if (!drain_retired_) drain_retired_ = now_ns();
       if (kernel_running()) break;
       const uint64_t t_upd = now_ns();
+      const NvtxRange nvtx_("bingo serve update");
       int st = BINGO_OK;
       const uint64_t k = r->a.size();
       for (uint64_t o = 0; o < k; o += cfg_.max_update_batch) {

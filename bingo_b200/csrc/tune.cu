@@ -31,6 +31,7 @@ double median(std::vector<double> v) {
 }  // namespace
 
 void Engine::autotune(const bingo_tune_request& R, bingo_tune_report* out) {
+  const NvtxRange nvtx_("bingo autotune");
   require_loaded();
   require_idle();
   if (!R.n_jobs && !R.n_ins && !R.n_del) throw Error(BINGO_ERR_INVALID_ARGUMENT, "empty tuning request");

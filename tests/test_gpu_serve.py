@@ -107,3 +107,39 @@ def test_admission_by_budget_and_busy_guard():
         assert np.array_equal(out, ex.walk(DEEPWALK, 80, np.full(2000, i, np.uint32), seed=i, job_id=i))
     g.serve_stop()
     g.walk(app=DEEPWALK, length=8, starts=[0])  # usable again
+
+
+def test_stalled_producer_and_bad_update():
+    """Failure handling without a GPU fault: when the producer stalls past the
+    idle limit, the serving kernel's bounded wait ends and the kernel exits
+    (the next query relaunches it and still gets exact rows); a malformed
+    update fails only its own ticket."""
+    import time
+    n, src, dst, w = _graph(scale=11, seed=97)
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    ref = Graph()
+    ref.load_edges(src, dst, w, n)
+    g.serve_start(idle_timeout_us=2000)
+    rng = np.random.default_rng(98)
+    st1 = rng.integers(0, n, size=300).astype(np.uint32)
+    t, out1 = g.submit_walk(app=DEEPWALK, length=30, starts=st1, seed=1, job_id=1)
+    assert g.serve_wait(t)["status"] == 0
+    l1 = g.serve_metrics()["walk_kernel_launches"]
+    time.sleep(0.05)  # the producer stalls for 25x the idle limit
+    st2 = rng.integers(0, n, size=300).astype(np.uint32)
+    t2, out2 = g.submit_walk(app=DEEPWALK, length=30, starts=st2, seed=2, job_id=2)
+    assert g.serve_wait(t2)["status"] == 0
+    # a still-running kernel would have taken this query without a launch
+    assert g.serve_metrics()["walk_kernel_launches"] == l1 + 1
+    bad = np.array([0, n + 7], np.uint32)
+    tb, _ = g.submit_update("insert", bad, np.array([1, 2], np.uint32), np.array([3, 4], np.uint32))
+    st3 = rng.integers(0, n, size=300).astype(np.uint32)
+    t3, out3 = g.submit_walk(app=DEEPWALK, length=30, starts=st3, seed=3, job_id=3)
+    assert g.serve_wait(tb)["status"] != 0  # OUT_OF_RANGE, nothing applied
+    assert g.serve_wait(t3)["status"] == 0
+    g.serve_stop()
+    assert np.array_equal(out3, ref.walk(app=DEEPWALK, length=30, starts=st3, seed=3, job_id=3))
+    assert np.array_equal(out1, ref.walk(app=DEEPWALK, length=30, starts=st1, seed=1, job_id=1))
+    assert np.array_equal(out2, ref.walk(app=DEEPWALK, length=30, starts=st2, seed=2, job_id=2))
+    assert g.stats()["live_edges"] == len(src)
