@@ -9,6 +9,7 @@ ids are 0-based. Errors raise `BingoError` carrying the C status.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 from dataclasses import dataclass
 from typing import Optional, Sequence
@@ -24,6 +25,14 @@ WALK_PPR_TAIL = 1
 BATCHED, PLAIN = 0, 1
 OP_WALK, OP_INSERT, OP_DELETE, OP_DELETE_PAIRS = 0, 1, 2, 3
 RUN_GRAPH = 1
+
+
+def _read_json(path) -> dict:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def _is_float(a) -> bool:
@@ -100,6 +109,7 @@ class Graph:
         cfg.device = device
         cfg.weight_mode = 1 if float_weights else 0
         self.float_weights = float_weights
+        self.device = device
         cfg.node2vec = 1 if node2vec else 0
         cfg.synchronous = 1 if synchronous else 0
         cfg.arena_factor = arena_factor
@@ -343,10 +353,43 @@ class Graph:
         t = BingoTuning(*[cur[f] for f in TUNING_FIELDS])
         self._check(self._L.bingo_set_tuning(self._h, ctypes.byref(t)))
 
-    def autotune(self, jobs: Sequence[WalkJob] = (), inserts=None, deletes=None, repeats: int = 3) -> dict:
+    def autotune(self, jobs: Sequence[WalkJob] = (), inserts=None, deletes=None, repeats: int = 3,
+                 cache: Optional[str] = None) -> dict:
         """Time the sample workload under candidate knobs and keep the fastest
         (bingo_autotune). inserts = (src, dst, w), deletes = (u, slot); the
-        update sample is undone, so the graph is unchanged."""
+        update sample is undone, so the graph is unchanged.
+
+        cache: a JSON file of tuned knobs keyed by GPU model and workload shape
+        (n, live edges, the jobs' apps / lengths / sizes, the update sizes);
+        a hit sets the stored knobs without timing anything ("cached": True)."""
+        key = None
+        if cache is not None:
+            key = self._tuning_key(jobs, inserts, deletes)
+            table = _read_json(cache)
+            if key in table:
+                self.set_tuning(**table[key])
+                return {"best": self.tuning(), "cached": True, "candidates": 0}
+        rep = self._autotune(jobs, inserts, deletes, repeats)
+        if cache is not None:
+            table = _read_json(cache)
+            table[key] = rep["best"]
+            tmp = f"{cache}.tmp{os.getpid()}"
+            with open(tmp, "w") as f:
+                json.dump(table, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache)
+        rep["cached"] = False
+        return rep
+
+    def _tuning_key(self, jobs, inserts, deletes) -> str:
+        import torch
+        st = self.stats()
+        size = lambda a: 0 if a is None else (a[0].numel() if hasattr(a[0], "numel") else len(a[0]))  # noqa: E731
+        shape = [(j.app, j.length, j.n_starts if j.starts is None else
+                  (j.starts.numel() if hasattr(j.starts, "numel") else len(j.starts))) for j in jobs]
+        return json.dumps([torch.cuda.get_device_name(self.device), st["n"], st["live_edges"], shape,
+                           size(inserts), size(deletes)])
+
+    def _autotune(self, jobs, inserts, deletes, repeats) -> dict:
         keep = []
         req = BingoTuneRequest()
         if jobs:

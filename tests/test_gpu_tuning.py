@@ -115,3 +115,23 @@ def test_invalid_tuning_rejected():
             g.set_tuning(**bad)
     with pytest.raises(ValueError):
         g.set_tuning(nonsense=1)
+
+
+def test_autotune_cache_reuses_knobs(tmp_path):
+    import json
+
+    import torch
+    n, src, dst, w, ops = workload(scale=11, ef=16, seed=43, rounds=1, k_ins=20000, k_del=20000)
+    cache = str(tmp_path / "tuning.json")
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    jobs = _jobs(n, np.random.default_rng(12), torch)
+    first = g.autotune(jobs, inserts=ops[0][1:4], deletes=ops[1][1:3], repeats=1, cache=cache)
+    assert not first["cached"] and first["candidates"] > 0
+    table = json.load(open(cache))
+    assert len(table) == 1 and list(table.values())[0] == first["best"]
+    h = Graph()  # a new handle on the same GPU and workload shape takes the stored knobs
+    h.load_edges(src, dst, w, n)
+    h.set_tuning(walk_chunk=128)
+    again = h.autotune(jobs, inserts=ops[0][1:4], deletes=ops[1][1:3], repeats=1, cache=cache)
+    assert again["cached"] and again["candidates"] == 0 and h.tuning() == first["best"]
