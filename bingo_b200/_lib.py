@@ -119,6 +119,14 @@ class BingoStats(ctypes.Structure):
     ]
 
 
+class BingoCheckReport(ctypes.Structure):
+    _fields_ = [(f, c_uint64) for f in ("vertices", "live_edges", "weight_sum", "members", "alias_slots",
+                                         "bad_vertices")] + [("kinds", c_uint32), ("first_bad", c_uint32)]
+
+
+CHECK_KINDS = {1: "extent", 2: "count", 4: "member", 8: "alias", 16: "hash", 32: "range"}
+
+
 # Every symbol include/bingo.h and include/bingo_gen.h declare, with its
 # ctypes signature (restype, argtypes).
 SIGNATURES = {
@@ -147,6 +155,7 @@ SIGNATURES = {
     "bingo_serve_get_metrics": (c_int, [c_void_p, POINTER(BingoServeMetrics)]),
     "bingo_save": (c_int, [c_void_p, ctypes.c_char_p]),
     "bingo_restore": (c_int, [c_void_p, ctypes.c_char_p]),
+    "bingo_check": (c_int, [c_void_p, POINTER(BingoCheckReport)]),
     "bingo_get_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
     "bingo_set_tuning": (c_int, [c_void_p, POINTER(BingoTuning)]),
     "bingo_autotune": (c_int, [c_void_p, POINTER(BingoTuneRequest), POINTER(BingoTuneReport)]),
@@ -201,6 +210,7 @@ STATUS = {
     9: "BINGO_ERR_NO_DEVICE",
     10: "BINGO_ERR_UNSUPPORTED",
     11: "BINGO_ERR_BUSY",
+    12: "BINGO_ERR_CORRUPT",
 }
 
 

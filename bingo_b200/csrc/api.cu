@@ -181,6 +181,11 @@ int bingo_restore(bingo_handle* h, const char* path) {
   return guarded(h, [&](bingo::Engine& e) { e.restore(path); });
 }
 
+int bingo_check(bingo_handle* h, bingo_check_report* out) {
+  if (!out) return BINGO_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&](bingo::Engine& e) { e.check(out); });
+}
+
 int bingo_get_tuning(bingo_handle* h, bingo_tuning* out) {
   if (!out) return BINGO_ERR_INVALID_ARGUMENT;
   return guarded(

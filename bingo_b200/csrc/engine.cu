@@ -567,7 +567,7 @@ Engine::~Engine() {
   DevBuf* bufs[] = {&vrec_, &meta_, &gdesc_, &gs_, &in_a_, &in_b_, &in_c_, &key_s_, &perm_, &iota_, &sa_,
                     &sb_, &head_, &seg_, &nseg_, &need_, &scan_, &base_, &ctl_, &slots_, &cub_tmp_, &jobs_,
                     &prefix_, &queue_, &wstart_, &wout_[0], &wout_[1], &pair_key_, &pair_key_s_, &pair_slot_,
-                    &fw_in_, &fw_fixed_};
+                    &fw_in_, &fw_fixed_, &check_buf_, &check_big_};
   for (DevBuf* b : bufs) b->release();
   for (int k = 0; k < 2; ++k) {
     if (walk_ev_[k]) cudaEventDestroy(walk_ev_[k]);
@@ -2030,6 +2030,7 @@ void Engine::restore(const char* path) {
                                                   : "snapshot has no node2vec adjacency index; create the handle with "
                                                     "config.node2vec = 0");
   if (!H.n) throw Error(BINGO_ERR_INVALID_ARGUMENT, "snapshot with n = 0");
+  if (!H.node2vec && H.top[A_HASH]) throw Error(BINGO_ERR_INVALID_ARGUMENT, "corrupt snapshot header");
   uint64_t expect = (uint64_t)H.n * (sizeof(VertexRec) + sizeof(VertexMeta) + kBits * sizeof(GroupDesc));
   for (int a = 0; a < kArenas; ++a) {
     if (H.top[a] > kArenaLimit[a]) throw Error(BINGO_ERR_INVALID_ARGUMENT, "corrupt snapshot header");
@@ -2092,7 +2093,14 @@ void Engine::restore(const char* path) {
   cuda_check(cudaMemcpyAsync(d_top_, h_top_, kArenas * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_),
              "restore");
   cuda_check(cudaMemsetAsync(d_err_, 0, 2 * sizeof(uint32_t), stream_), "restore");
-  cuda_check(cudaStreamSynchronize(stream_), "restore");
+  // The checksum only shows the file is the one written; the store check
+  // shows its content is a store the kernels can index safely.
+  bingo_check_report rep{};
+  check_store(&rep);
+  if (rep.bad_vertices)
+    throw Error(BINGO_ERR_CORRUPT, "snapshot content fails the store check: " + std::to_string(rep.bad_vertices) +
+                                       " vertices, first " + std::to_string(rep.first_bad) + ", kinds " +
+                                       std::to_string(rep.kinds));
   loaded_ = true;
 }
 

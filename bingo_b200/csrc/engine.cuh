@@ -93,6 +93,7 @@ class Engine {
   void philox_batch(const uint32_t* ctr4, uint64_t count, uint64_t key, uint32_t* out4);
   void save(const char* path);
   void restore(const char* path);
+  void check(bingo_check_report* out);  // throws BINGO_ERR_CORRUPT after filling *out
   const Tuning& tuning() const { return tuning_; }
   void set_tuning(const Tuning& t);
   void autotune(const bingo_tune_request& req, bingo_tune_report* out);
@@ -144,6 +145,7 @@ class Engine {
       slots_, cub_tmp_;
   DevBuf pair_key_, pair_key_s_, pair_slot_;  // delete-by-pair translation
   DevBuf fw_in_, fw_fixed_;                   // float weights: staged input, 16.16 fixed point
+  DevBuf check_buf_, check_big_;              // store check: totals, large-vertex list
   uint64_t iota_n_ = 0;
   // walk scratch
   DevBuf jobs_, prefix_, queue_, wstart_;
@@ -185,6 +187,7 @@ class Engine {
   void ensure_pair_scratch(uint64_t k);
   void translate_pairs(const uint32_t* du, const uint32_t* dv, uint64_t k);
   void check_batch_on_device(const uint32_t* a, const uint32_t* b, const uint32_t* w, uint64_t k);
+  void check_store(bingo_check_report* out);
   bool save_state(StateCopy& c);
   void restore_state(const StateCopy& c);
 };

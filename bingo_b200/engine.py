@@ -16,8 +16,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import (TUNING_FIELDS, BingoConfig, BingoError, BingoOp, BingoServeConfig, BingoServeMetrics,
-                   BingoServeStatus, BingoStats, BingoTuneReport, BingoTuneRequest, BingoTuning, BingoWalkJob, lib)
+from ._lib import (CHECK_KINDS, TUNING_FIELDS, BingoCheckReport, BingoConfig, BingoError, BingoOp,
+                   BingoServeConfig, BingoServeMetrics, BingoServeStatus, BingoStats, BingoTuneReport, BingoTuneRequest, BingoTuning, BingoWalkJob, lib)
 
 DEEPWALK, NODE2VEC, PPR, SAMPLING = 0, 1, 2, 3
 APPS = {"deepwalk": DEEPWALK, "node2vec": NODE2VEC, "ppr": PPR, "sampling": SAMPLING}
@@ -335,6 +335,21 @@ class Graph:
         """Replace this handle's graph with a saved one (bingo_restore)."""
         self._check(self._L.bingo_restore(self._h, os.fsencode(path)))
         self.n = self.stats()["n"]
+
+    # ------------------------------------------------------------ store check
+    def check(self, raise_on_corrupt: bool = True) -> dict:
+        """Verify every structural invariant of the graph store on the device
+        (bingo_check): extents, live and group counts, group members and
+        back-pointers, exact alias tables, the adjacency index, neighbour
+        ranges. Returns the report; a failing store raises
+        BingoError(BINGO_ERR_CORRUPT) unless raise_on_corrupt is false."""
+        r = BingoCheckReport()
+        st = self._L.bingo_check(self._h, ctypes.byref(r))
+        rep = {f: getattr(r, f) for f, _ in BingoCheckReport._fields_}
+        rep["kind_names"] = [name for bit, name in CHECK_KINDS.items() if r.kinds & bit]
+        if st and not (st == 12 and not raise_on_corrupt):
+            self._check(st)
+        return rep
 
     # ------------------------------------------------------------ tuning
     def tuning(self) -> dict:

@@ -42,7 +42,8 @@ typedef enum bingo_status {
   BINGO_ERR_TIMEOUT = 8,          /* a bounded device wait expired */
   BINGO_ERR_NO_DEVICE = 9,        /* no usable CUDA device */
   BINGO_ERR_UNSUPPORTED = 10,     /* e.g. node2vec without the adjacency index */
-  BINGO_ERR_BUSY = 11             /* the handle is serving; only bingo_serve_* calls are allowed */
+  BINGO_ERR_BUSY = 11,            /* the handle is serving; only bingo_serve_* calls are allowed */
+  BINGO_ERR_CORRUPT = 12          /* the graph store breaks an invariant (bingo_check; a restored snapshot) */
 } bingo_status;
 
 typedef enum bingo_app {
@@ -280,7 +281,51 @@ int bingo_serve_wait(bingo_handle* h, uint64_t ticket, uint64_t timeout_us, bing
  * file is checksummed and tied to this build's record layout and to
  * config.node2vec; a restore that fails leaves the handle with no graph. */
 int bingo_save(bingo_handle* h, const char* path);
+/* The restored store is checked as by bingo_check before the handle takes
+ * it; a file whose content breaks an invariant (with a valid checksum)
+ * returns BINGO_ERR_CORRUPT and leaves the handle with no graph. */
 int bingo_restore(bingo_handle* h, const char* path);
+
+/* ---- Store check ----------------------------------------------------------
+ * No reference counterpart (the reference has no consistency checker). One
+ * device pass over the whole store verifies every structural invariant the
+ * walk and update kernels rely on, reading each record only after the
+ * offsets that lead to it were checked against the used part of its arena
+ * (so a corrupt store yields a report, never an out-of-bounds access):
+ *   EXTENT  a vertex's edge slots, back-pointer pool, group lists, alias
+ *           table or adjacency index reach past the used part of its arena,
+ *           or a count exceeds its capacity;
+ *   COUNT   the live-slot count or a group's member count differs from the
+ *           live slots carrying that weight bit;
+ *   MEMBER  a group member names a slot that is not live, lacks the group's
+ *           bit or holds another neighbour, or its back-pointer disagrees;
+ *   ALIAS   the alias table is not the exact table over the group masses
+ *           cnt_k * 2^k (slot count, totals, own / alias groups, and for
+ *           every group the scaled mass its slots carry);
+ *   HASH    a live neighbour is missing from the adjacency index, or the
+ *           index's key, multiplicity or weight totals disagree;
+ *   RANGE   a live slot holds a neighbour id >= n.
+ * Returns BINGO_OK with a clean report, BINGO_ERR_CORRUPT with the report
+ * filled when any vertex fails. */
+enum {
+  BINGO_CHECK_EXTENT = 1,
+  BINGO_CHECK_COUNT = 2,
+  BINGO_CHECK_MEMBER = 4,
+  BINGO_CHECK_ALIAS = 8,
+  BINGO_CHECK_HASH = 16,
+  BINGO_CHECK_RANGE = 32
+};
+typedef struct bingo_check_report {
+  uint64_t vertices;       /* vertices checked (= n) */
+  uint64_t live_edges;     /* live (non-tombstone) edge slots */
+  uint64_t weight_sum;     /* sum of the live weights, modulo 2^64 */
+  uint64_t members;        /* group members over all vertices (= sum of popcount(w) over live slots) */
+  uint64_t alias_slots;    /* alias slots over all vertices (= nonzero groups) */
+  uint64_t bad_vertices;   /* vertices failing at least one check */
+  uint32_t kinds;          /* BINGO_CHECK_* bits seen */
+  uint32_t first_bad;      /* lowest failing vertex id, or 0xffffffff */
+} bingo_check_report;
+int bingo_check(bingo_handle* h, bingo_check_report* out);
 
 /* ---- Tuning -------------------------------------------------------------
  * Launch and batching parameters. None of them changes any result (walks,

@@ -1,7 +1,8 @@
 """Properties at the full size of the DeepWalk workload (R-MAT scale 20,
 16.1 M edges, log-uniform weights in [1, 2^20), 50K + 50K update batches,
 one walk of length 80 per vertex), where a full CPU-oracle replay would take
-minutes: counts add up, an insert followed by the delete of exactly its
+minutes: counts add up, the device store check is clean with totals equal
+to the live edge set, an insert followed by the delete of exactly its
 slots restores every group count, live degree and alias mass, every walk
 transition is a live edge, walks repeat exactly, and the batched launch
 equals the plain one."""
@@ -31,6 +32,17 @@ def _group_mass(d, n):
     return g, (g * (np.uint64(1) << np.arange(32, dtype=np.uint64))).sum(1)
 
 
+def _check_totals(g, live_weights):
+    """The device store check is clean and its totals match the live edge set."""
+    rep = g.check()
+    assert rep["bad_vertices"] == 0 and rep["kinds"] == 0
+    lw = live_weights.astype(np.uint64)
+    assert rep["live_edges"] == len(lw)
+    assert rep["weight_sum"] == int(lw.sum())
+    assert rep["members"] == int(np.unpackbits(lw.astype(np.uint32).view(np.uint8)).sum())
+    return rep
+
+
 def test_counts_and_round_trip(big):
     n, src, dst, w, g = big
     st = g.stats()
@@ -44,6 +56,7 @@ def test_counts_and_round_trip(big):
     slots = g.insert_batch(s, d, ww)
     st = g.stats()
     assert st["slots"] == len(src) + 50_000 and st["live_edges"] == len(src) + 50_000
+    _check_totals(g, np.concatenate([w, ww]))
     g.delete_batch(s, slots)  # the same edges again: a full round trip
     after = g.dump()
     st = g.stats()
@@ -59,6 +72,8 @@ def test_counts_and_round_trip(big):
     old = local < ecnt0[vert]
     assert np.array_equal(after["ev"][old], before["ev"]) and np.array_equal(after["ew"][old], before["ew"])
     assert (~old).sum() == 50_000 and (after["ew"][~old] == 0).all()
+    rep = _check_totals(g, w)
+    assert rep["alias_slots"] == int(after["am"].sum())
 
 
 def test_walk_transitions_live_and_repeatable(big):
