@@ -3,7 +3,7 @@
 // randomWalk) rewritten over the C ABI of libbingo.so.
 //
 //   bingo_driver [d|n|p|s] [-g edge_list | -r scale] [-i|-d|-m] [-b batch]
-//                [-l len] [-k iterations] [-s seed] [-o] [-f]
+//                [-l len] [-k iterations] [-s seed] [-o] [-f] [-c]
 //
 // d / n / p / s: DeepWalk, node2vec, PPR, one-hop sampling (default d).
 // -g: a "u v" edge-list file (the reference reads ../dataset/<name>);
@@ -15,7 +15,9 @@
 // -b: batch size (default 100000); -l: walk length (default 80); -k:
 //     iterations of {update, walk} (default 10); -s: seed; -o: print the
 //     first 10 walks; -f: float weights (the reference's wtype::Float: the
-//     integer weight plus a random hundredth, inserts too).
+//     integer weight plus a random hundredth, inserts too); -c: run the
+//     store check (bingo_check) after the load and after every iteration's
+//     updates, outside the timed regions, and stop on the first failure.
 //
 // Updates follow the reference: an insert batch copies random existing
 // (u, v) pairs (parallel edges allowed) and a delete batch removes random
@@ -75,7 +77,7 @@ int main(int argc, char** argv) {
   int scale = 0;
   uint64_t batch = 100000, iters = 10, seed = 1;
   uint32_t len = 80;
-  bool print_paths = false, float_w = false;
+  bool print_paths = false, float_w = false, store_check = false;
   int pos = 1;
   if (pos < argc && argv[pos][0] != '-') {
     switch (argv[pos][0]) {
@@ -104,6 +106,7 @@ int main(int argc, char** argv) {
     else if (a == "-s") seed = std::strtoull(val(), nullptr, 10);
     else if (a == "-o") print_paths = true;
     else if (a == "-f") float_w = true;
+    else if (a == "-c") store_check = true;
     else {
       std::fprintf(stderr, "bingo_driver: unknown option %s\n", a.c_str());
       return 1;
@@ -171,6 +174,19 @@ int main(int argc, char** argv) {
   } else {
     check(h, bingo_load_edges(h, src.data(), dst.data(), w.data(), m, n), "load");
   }
+  uint64_t checks = 0;
+  auto check_store = [&](const char* when) {
+    if (!store_check) return;
+    bingo_check_report rep;
+    const int rc = bingo_check(h, &rep);
+    if (rc != BINGO_OK) {
+      std::fprintf(stderr, "bingo_driver: store check after %s failed (status %d): %llu bad vertices, first %u, "
+                   "kinds %u\n", when, rc, (unsigned long long)rep.bad_vertices, rep.first_bad, rep.kinds);
+      std::exit(3);
+    }
+    ++checks;
+  };
+  check_store("the load");
   std::vector<EdgeData> edges(m);
   {
     std::vector<uint32_t> next_slot(n, 0);
@@ -223,6 +239,7 @@ int main(int argc, char** argv) {
       live -= batch;
       updates += batch;
     }
+    check_store("an update iteration");
     bingo_walk_job j;
     std::memset(&j, 0, sizeof j);
     j.app = app;
@@ -251,10 +268,10 @@ int main(int argc, char** argv) {
   std::printf(
       "{\"app\": %d, \"n\": %u, \"m\": %llu, \"iterations\": %llu, \"batch\": %llu, \"walk_s\": %.6f, "
       "\"update_s\": %.6f, \"eval_s\": %.6f, \"walk_steps\": %llu, \"walk_steps_per_s\": %.1f, "
-      "\"edge_updates_per_s\": %.1f, \"live_edges\": %llu, \"total_s\": %.6f}\n",
+      "\"edge_updates_per_s\": %.1f, \"live_edges\": %llu, \"store_checks\": %llu, \"total_s\": %.6f}\n",
       app, n, (unsigned long long)m, (unsigned long long)iters, (unsigned long long)batch, t_walk, t_update,
       t_eval, (unsigned long long)steps, t_walk > 0 ? steps / t_walk : 0.0, t_update > 0 ? updates / t_update : 0.0,
-      (unsigned long long)st.live_edges, now_s() - t_total0);
+      (unsigned long long)st.live_edges, (unsigned long long)checks, now_s() - t_total0);
   bingo_destroy(h);
   return 0;
 }

@@ -1,6 +1,7 @@
 """The C++ experiment driver (bingo_b200/bingo_driver, the reference's
-instance() over the C ABI): runs every app and update mode on the GPU, reads
-an edge-list file, and fails with a clear status when there is no GPU."""
+instance() over the C ABI): runs every app and update mode on the GPU (with
+the store check after every iteration on request), reads an edge-list file,
+and fails with a clear status when there is no GPU."""
 import json
 import os
 import subprocess
@@ -29,7 +30,7 @@ def test_driver_without_gpu_reports_status():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("app,mode,extra", [("d", "-m", []), ("n", "-i", []), ("p", "-d", []), ("s", "-m", []),
-                                            ("d", "-m", ["-f"])])
+                                            ("d", "-m", ["-f"]), ("n", "-m", ["-c"])])
 def test_driver_runs_the_reference_loop(app, mode, extra):
     r = _run(app, "-r", "12", mode, "-b", "4000", "-k", "3", "-l", "40", *extra)
     assert r.returncode == 0, r.stderr
@@ -39,6 +40,7 @@ def test_driver_runs_the_reference_loop(app, mode, extra):
     want = d["m"] + (per if mode in ("-m", "-i") else 0) - (per if mode in ("-m", "-d") else 0)
     assert d["live_edges"] == want
     assert d["walk_steps"] > 0 and d["walk_steps_per_s"] > 0
+    assert d["store_checks"] == (1 + d["iterations"] if "-c" in extra else 0)
 
 
 @pytest.mark.gpu

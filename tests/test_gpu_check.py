@@ -298,7 +298,7 @@ def test_large_vertex_damage(tmp_path):
     """A vertex with more than 4096 group members is checked by a whole CTA;
     damage there is reported once, merged with the vertex's other results."""
     n, src, dst, w, _ = workload(scale=13, ef=16, seed=8, dist=gen.W_LOGUNIFORM, lo=1, hi=2 ** 31, rounds=0)
-    g, ex = Graph(), po.ExactGraph(n)
+    g, ex = Graph(node2vec=False), po.ExactGraph(n)
     g.load_edges(src, dst, w, n)
     ex.load(src, dst, w)
     path = tmp_path / "big.snap"
@@ -318,7 +318,7 @@ def test_large_vertex_damage(tmp_path):
     # bad vertex carrying both kinds
     s.set_u32("meta", u * s.rec[1] + 32, s.meta(u)[6] - 1)
     s.write(bad)
-    h = Graph()
+    h = Graph(node2vec=False)
     with pytest.raises(BingoError) as e:
         h.restore(bad)
     assert e.value.name == "BINGO_ERR_CORRUPT"
