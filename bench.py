@@ -584,10 +584,14 @@ def measure_engine(args, n, src, dst, w, batches, local, app=None, length=WALK_L
     upd = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(args.warmup, total)) / 1e3
     wlk = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
     whole = sum(ev[i][0].elapsed_time(ev[i][2]) for i in range(args.warmup, total)) / 1e3
+    chk = g.check(raise_on_corrupt=False)  # after the timed steps: the store they left is sound
     g.close()
+    if chk["bad_vertices"]:
+        raise SystemExit(f"bench: the graph store fails its check after the timed updates: {chk}")
     r = {"value": steps / whole, "walk_steps_per_s": steps / wlk, "edge_updates_per_s": upd_edges / upd,
          "walk_kernel_ms_per_step": wlk * 1e3 / args.steps, "update_ms_per_step": upd * 1e3 / args.steps,
-         "steps_per_walk_phase": steps / args.steps}
+         "steps_per_walk_phase": steps / args.steps,
+         "store_check": {"bad_vertices": chk["bad_vertices"], "live_edges": chk["live_edges"]}}
     if app == NODE2VEC:
         trials = s1["walk_trials"] - s0["walk_trials"]
         probes = s1["walk_probes"] - s0["walk_probes"]
@@ -789,6 +793,15 @@ def run_ours(args):
         e2e = run_e2e(args, g, n, src, dst, w, batches, seed, stream, dev, world)
     clk = clocks.stop(t_busy0, time.time())
 
+    # ---- the store the timed updates left behind: every invariant holds
+    # (bingo_check, outside every timed region); a failing store voids the run
+    t_chk = time.perf_counter()
+    chk = g.check(raise_on_corrupt=False)
+    store_check = {"bad_vertices": chk["bad_vertices"], "kinds": chk["kind_names"],
+                   "live_edges": chk["live_edges"], "ms": (time.perf_counter() - t_chk) * 1e3}
+    if chk["bad_vertices"]:
+        raise SystemExit(f"bench: the graph store fails its check after the timed updates: {store_check}")
+
     # ---- roofline of the walk kernel
     peak, peak_src = peak_hbm()
     achieved = steps_local * BYTES_PER_STEP / (walk_ms / 1e3) / 1e9
@@ -836,6 +849,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches) * world,
+            "store_check": store_check,
         }
         print(json.dumps(line), flush=True)
     g.close()

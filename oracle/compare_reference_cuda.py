@@ -5,12 +5,15 @@ compiled by `make -C oracle ref`, see ref_harness.cu) as a measured
 baseline, then this engine through bench.py's measure_engine on the same
 graph and batches. The product never runs anything here.
 
-    python oracle/compare_reference_cuda.py [--workload plain|node2vec] [--steps K] [--warmup W]
+    python oracle/compare_reference_cuda.py [--workload plain|node2vec|small] [--steps K] [--warmup W]
 
 plain: DeepWalk on R-MAT 20 with weights log-uniform in [1, 2^16) (the
 reference's MAXLOG = 16) and 50K + 50K update batches; node2vec: R-MAT 22,
 Zipf weights below 2^16, 1M-edge batches, walk length 80 (the reference's
-compile-time LEN). Prints one JSON line.
+compile-time LEN); small: DeepWalk on R-MAT 14 (16,384 vertices, edge factor
+16) with weights uniform in [1, 1024] and 10K + 10K update batches, one walk
+of length 80 per vertex (its whole state fits in L2, so this measures launch
+and L2-resident work, not HBM). Prints one JSON line.
 """
 import argparse
 import json
@@ -27,6 +30,21 @@ from bench import (BATCH_DEL, BATCH_INS, EDGE_FACTOR, N_BATCH, N_SCALE, SCALE, W
                    dist_setup, make_node2vec_workload, make_workload, measure_engine)
 
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
+
+SMALL = dict(scale=14, ef=16, seed=1235, lo=1, hi=1024, k=10_000)
+
+
+def make_small_workload(steps_total):
+    """R-MAT 14, uniform [1, 1024] weights, 10K absent-pair inserts + 10K
+    live-edge deletes per step (the parity tests' small DeepWalk case)."""
+    from bingo_b200 import gen
+    n = 1 << SMALL["scale"]
+    src, dst = gen.rmat(SMALL["scale"], SMALL["ef"], seed=SMALL["seed"])
+    w = gen.weights(len(src), gen.W_UNIFORM, SMALL["lo"], SMALL["hi"], seed=SMALL["seed"] + 1)
+    ug = gen.UpdateGen(n, src, dst, seed=SMALL["seed"] + 2)
+    batches = [(ug.inserts(SMALL["k"], gen.W_UNIFORM, SMALL["lo"], SMALL["hi"]), ug.deletes(SMALL["k"]))
+               for _ in range(steps_total)]
+    return n, src, dst, w, batches
 
 
 def run_reference_cuda(args):
@@ -51,6 +69,8 @@ def run_reference_cuda(args):
     n2v = args.workload == "node2vec"
     if n2v:  # node2vec on R-MAT 22 within the reference's limits: weights < 2^16 (MAXLOG), its fixed LEN = 80
         n, src, dst, w, batches = make_node2vec_workload(total, w_hi=w_hi - 1)
+    elif args.workload == "small":
+        n, src, dst, w, batches = make_small_workload(total)
     else:
         n, src, dst, w, batches = make_workload(total, w_hi=w_hi)
     with tempfile.TemporaryDirectory() as td:
@@ -92,6 +112,11 @@ def run_reference_cuda(args):
                "note": "walk length 80 = the reference's compile-time LEN (include/api.h:12); its node2vec tests "
                        "prev in N(cur) with a load-time hash (include/operation.cuh:313), so its step counts "
                        "and acceptance differ from the exact node2vec here"}
+    elif args.workload == "small":
+        ours = measure_engine(args, n, src, dst, w, batches, local)
+        cfg = {"workload": "plain-deepwalk-rmat14", "scale": SMALL["scale"], "edge_factor": SMALL["ef"],
+               "weights": "uniform[1,1024]", "walks": n, "walk_len": WALK_LEN,
+               "batch": {"insert": SMALL["k"], "delete": SMALL["k"]}, "l2": "whole state L2-resident"}
     else:
         ours = measure_engine(args, n, src, dst, w, batches, local)
         cfg = {"workload": WORKLOAD + "-w16", "scale": SCALE, "edge_factor": EDGE_FACTOR,
@@ -105,7 +130,7 @@ def run_reference_cuda(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="plain", choices=["plain", "node2vec"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "node2vec", "small"])
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     run_reference_cuda(ap.parse_args())
