@@ -155,6 +155,13 @@ def barrier(world: int):
 
 
 # --------------------------------------------------------------------------- CPU leg
+CPU_WALK_FORM = "OpenMP over all host threads, 16 walks per thread in flight"
+
+
+def scaled_note(walks, n):
+    return "" if walks >= n else f", walk time scaled to {n} walks"
+
+
 class CpuRun:
     """The CPU oracle (OpenMP, all host threads) on the same graph: load once,
     then per step one full update batch and a bounded walk sample."""
@@ -175,7 +182,10 @@ class CpuRun:
         rng = np.random.default_rng(seed)
         starts = np.sort(rng.choice(self.n, size=walks, replace=False)).astype(np.uint32)
         t0 = time.perf_counter()
-        rows = self.ex.walk(app, length, starts, seed=seed, job_id=0, p=p, q=q)
+        if app in (0, 2):  # DeepWalk / PPR: several walks per thread in flight, the same rows as walk()
+            rows = self.ex.walk_interleaved(app, length, starts, seed=seed, job_id=0)
+        else:
+            rows = self.ex.walk(app, length, starts, seed=seed, job_id=0, p=p, q=q)
         t_walk = time.perf_counter() - t0
         steps = int((rows >= 0).sum() - len(starts))
         scale = self.n / walks  # extrapolate the walk sample to one walk per vertex
@@ -193,7 +203,7 @@ def run_reference(args):
     if rank != 0:
         return
     n, src, dst, w, batches = make_workload(args.warmup + args.steps)
-    walks = args.ref_walks
+    walks = min(args.ref_walks, n)
     vals, last = [], None
     cpu = CpuRun(n, src, dst, w)
     for i in range(args.warmup + args.steps):
@@ -210,8 +220,8 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "weights": "loguniform[1,2^20)",
                    "walks": n, "walk_len": WALK_LEN, "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
-                         "sample": f"per step: one full 50K+50K update batch + {walks} walks x {WALK_LEN}, "
-                                   f"walk time scaled to {n} walks"},
+                         "sample": f"per step: one full 50K+50K update batch + {walks} walks x {WALK_LEN} "
+                                   f"(oracle port, {CPU_WALK_FORM})" + scaled_note(walks, n)},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "walk_steps_per_s": last["walk_steps_per_s"], "edge_updates_per_s": last["edge_updates_per_s"],
     }
@@ -602,6 +612,7 @@ def measure_engine(args, n, src, dst, w, batches, local, app=None, length=WALK_L
 
 # --------------------------------------------------------------------------- node2vec on R-MAT 22
 N_SCALE, N_LEN, N_BATCH = 22, 40, 1_000_000
+N_CPU_WALKS = 131072
 N_SEED = 1234 + 3
 N2V_BYTES_PER_TRIAL, N2V_BYTES_PER_PROBE = 32, 8  # algorithmic bytes: one alias draw; one adjacency lookup
 
@@ -634,7 +645,7 @@ def run_node2vec(args):
     peak, peak_src = peak_hbm()
     cpu = None
     if not args.no_cpu:
-        walks = min(args.cpu_walks, n)
+        walks = min(args.cpu_walks, N_CPU_WALKS)  # node2vec runs the plain oracle walk: a smaller sample
         c = CpuRun(n, src, dst, w).step(batches[0], walks, seed=7, app=NODE2VEC, length=N_LEN, p=0.5, q=2.0)
         cpu = {"value": c["value"], "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"one full 500K+500K update batch + {walks} node2vec walks x {N_LEN} on the CPU oracle "
@@ -824,10 +835,10 @@ def run_ours(args):
         roof["random_sector_ceiling"] = pr
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = CpuRun(n, src, dst, w).step(batches[0], args.cpu_walks, seed=7)
+        r = CpuRun(n, src, dst, w).step(batches[0], min(args.cpu_walks, n), seed=7)
         cpu = {"value": r["value"], "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"one full 50K+50K update batch + {args.cpu_walks} walks x {WALK_LEN} on the CPU oracle "
-                         f"(OpenMP), walk time scaled to {n} walks",
+               "sample": f"one full 50K+50K update batch + {min(args.cpu_walks, n)} walks x {WALK_LEN} on the CPU "
+                         f"oracle ({CPU_WALK_FORM})" + scaled_note(args.cpu_walks, n),
                "walk_steps_per_s": r["walk_steps_per_s"], "edge_updates_per_s": r["edge_updates_per_s"]}
 
     if rank == 0:
@@ -875,8 +886,8 @@ def main():
     ap.add_argument("--requests", type=int, default=400, help="served: requests per rate")
     ap.add_argument("--p-update", type=float, default=0.05, help="served: fraction of update requests")
     ap.add_argument("--serve-budget", type=int, default=4096, help="served: output budget in MiB")
-    ap.add_argument("--cpu-walks", type=int, default=131072)
-    ap.add_argument("--ref-walks", type=int, default=131072)
+    ap.add_argument("--cpu-walks", type=int, default=1 << 20)
+    ap.add_argument("--ref-walks", type=int, default=1 << 20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-gather-ceiling", action="store_true",

@@ -32,6 +32,7 @@
 #pragma once
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -408,6 +409,114 @@ struct ExactGraph {
         if (app == APP_PPR && (uint64_t)philox4x32_10(U4{i, j, 1, job}, k0, k1).x < th.stop) break;
       }
       for (uint32_t j = pos + 1; j < L; ++j) row[j] = -1;
+    }
+  }
+
+  // The same DeepWalk and PPR walks as walk() (PPR without the tail flag),
+  // bit for bit, arranged for speed: each thread advances kLanes walks in
+  // turn, one dependent read per visit (vertex record, alias slot, group,
+  // member), and prefetches the next read of a walk before moving to the
+  // next one, so a thread keeps kLanes cache misses in flight instead of
+  // one. This is the timed CPU baseline; walk() stays the checker.
+  void walk_interleaved(int app, uint32_t L, const uint32_t* starts, uint64_t n_starts, uint64_t seed, uint32_t job,
+                        double stop, int32_t* out) const {
+    constexpr int kLanes = 16;
+    enum Stage { S_FREE, S_VERT, S_ALIAS, S_GROUP, S_MEMBER };
+    struct Lane {
+      int stage = S_FREE;
+      uint32_t i = 0, j = 0, cur = 0, slot = 0, idx = 0;
+      int32_t* row = nullptr;
+      const Vertex* X = nullptr;
+      const Group* G = nullptr;
+      U4 r{};
+    };
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const uint64_t thr_stop = prob_threshold(stop);
+    const bool ppr = app == APP_PPR;
+    std::atomic<uint64_t> next{0};
+#pragma omp parallel
+    {
+      Lane lane[kLanes];
+      int busy = 0;
+      bool drained = false;
+      // Ends walk l after writing row[pos]: the rest of the row is -1.
+      auto finish = [&](Lane& w, uint32_t pos) {
+        for (uint32_t j = pos + 1; j < L; ++j) w.row[j] = -1;
+        w.stage = S_FREE;
+        --busy;
+      };
+      for (;;) {
+        for (int l = 0; l < kLanes; ++l) {
+          Lane& w = lane[l];
+          switch (w.stage) {
+            case S_FREE: {
+              if (drained) break;
+              const uint64_t i = next.fetch_add(1, std::memory_order_relaxed);
+              if (i >= n_starts) {
+                drained = true;
+                break;
+              }
+              w.i = (uint32_t)i;
+              w.row = out + i * L;
+              if (L == 0) break;
+              w.cur = starts[i];
+              w.row[0] = (int32_t)w.cur;
+              if (L == 1) break;
+              w.j = 1;
+              w.stage = S_VERT;
+              ++busy;
+              __builtin_prefetch(&vx[w.cur].m);
+              break;
+            }
+            case S_VERT: {
+              w.X = &vx[w.cur];
+              if (!w.X->m) {
+                w.row[w.j] = -1;
+                finish(w, w.j);
+                break;
+              }
+              w.r = philox4x32_10(U4{w.i, w.j, 0, job}, k0, k1);
+              w.slot = mulhi32(w.r.x, (uint32_t)w.X->m);
+              __builtin_prefetch(&w.X->alias[w.slot]);
+              __builtin_prefetch(&w.X->gl);
+              w.stage = S_ALIAS;
+              break;
+            }
+            case S_ALIAS: {
+              const AliasSlot& A = w.X->alias[w.slot];
+              const uint64_t d = mulhi64(((uint64_t)w.r.y << 32) | w.r.z, A.T);
+              w.G = w.X->gptr(d < A.thr ? A.own : A.alias);
+              __builtin_prefetch(w.G);
+              w.stage = S_GROUP;
+              break;
+            }
+            case S_GROUP: {
+              w.idx = mulhi32(w.r.w, (uint32_t)w.G->v.size());
+              __builtin_prefetch(w.G->v.data() + w.idx);
+              w.stage = S_MEMBER;
+              break;
+            }
+            case S_MEMBER: {
+              const uint32_t x = w.G->v[w.idx];
+              w.row[w.j] = (int32_t)x;
+              w.cur = x;
+              if (ppr && (uint64_t)philox4x32_10(U4{w.i, w.j, 1, job}, k0, k1).x < thr_stop) {
+                finish(w, w.j);
+                break;
+              }
+              if (++w.j >= L) {
+                w.stage = S_FREE;
+                --busy;
+                break;
+              }
+              __builtin_prefetch(&vx[x].m);
+              w.stage = S_VERT;
+              break;
+            }
+          }
+        }
+        if (drained && busy == 0) break;
+      }
     }
   }
 };

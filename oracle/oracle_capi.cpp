@@ -50,6 +50,12 @@ void orc_walk(void* g, int app, uint32_t L, const uint32_t* starts, uint64_t n_s
               double p, double q, double stop, uint32_t flags, int32_t* out) {
   ((const ExactGraph*)g)->walk(app, L, starts, n_starts, seed, job, p, q, stop, flags, out);
 }
+// DeepWalk / PPR (no tail flag) with several walks per thread in flight:
+// the same rows as orc_walk, faster (the timed CPU baseline).
+void orc_walk_interleaved(void* g, int app, uint32_t L, const uint32_t* starts, uint64_t n_starts, uint64_t seed,
+                          uint32_t job, double stop, int32_t* out) {
+  ((const ExactGraph*)g)->walk_interleaved(app, L, starts, n_starts, seed, job, stop, out);
+}
 int orc_has_edge(void* g, uint32_t u, uint32_t v) {
   const ExactGraph* G = (const ExactGraph*)g;
   return G->adj_has(G->vx[u], v);
