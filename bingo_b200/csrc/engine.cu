@@ -1567,14 +1567,38 @@ struct NoAllocScratch {
 };
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
+// The call's job table and walk offsets travel as one kernel parameter
+// (values, not a pointer to host memory; 6,404 bytes, under the 32,764-byte
+// parameter limit), and this kernel writes them into the scratch and zeroes
+// the work counter, ahead of the walk launch on the same stream.
+struct NoAllocJobs {
+  WalkJobDev jobs[kNoAllocMaxJobs];
+  uint32_t prefix[kNoAllocMaxJobs + 1];
+  uint32_t n_jobs;
+};
+static_assert(sizeof(NoAllocJobs) <= 32764, "kernel parameter limit");
+
+__global__ void k_noalloc_stage(const __grid_constant__ NoAllocJobs in, NoAllocScratch* dst) {
+  const uint32_t words = (uint32_t)(in.n_jobs * sizeof(WalkJobDev) / 4);
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(in.jobs);
+  uint32_t* out = reinterpret_cast<uint32_t*>(dst->jobs);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) out[i] = src[i];
+  for (uint32_t i = threadIdx.x; i <= in.n_jobs; i += blockDim.x) dst->prefix[i] = in.prefix[i];
+  if (threadIdx.x == 0) dst->queue = 0;
+}
+static_assert(sizeof(WalkJobDev) % 4 == 0, "word copy");
+
 namespace {
+constexpr int kNoAllocMaxDevices = 128;
 std::mutex g_noalloc_mu;
-NoAllocScratch* g_noalloc_ptr[128] = {};
+NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch for `device` (must be current); looked up
-// once per device.
+// once per device. The ordinal is checked before it indexes the table.
 NoAllocScratch* noalloc_scratch(int device) {
-  if (device < 0 || device >= 128) throw Error(BINGO_ERR_INVALID_ARGUMENT, "device ordinal above 127");
+  if (device < 0 || device >= kNoAllocMaxDevices)
+    throw Error(BINGO_ERR_INVALID_ARGUMENT, "bingo_walk_noalloc supports device ordinals 0.." +
+                                                std::to_string(kNoAllocMaxDevices - 1));
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_ptr[device]) {
     void* p = nullptr;
@@ -1594,8 +1618,10 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
     throw Error(BINGO_ERR_INVALID_ARGUMENT, "bingo_walk_noalloc takes at most " + std::to_string(kNoAllocMaxJobs) +
                                                 " jobs per call (got " + std::to_string(n_jobs) + ")");
   NoAllocScratch* scratch = noalloc_scratch(cfg_.device);
-  WalkJobDev dj[kNoAllocMaxJobs];
-  uint32_t prefix[kNoAllocMaxJobs + 1];
+  NoAllocJobs in;
+  WalkJobDev* dj = in.jobs;
+  uint32_t* prefix = in.prefix;
+  in.n_jobs = n_jobs;
   prefix[0] = 0;
   uint64_t total = 0;
   for (uint32_t j = 0; j < n_jobs; ++j) {
@@ -1635,13 +1661,11 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
     D.out = J.out;
   }
   if (!total) return;
-  // The job table and prefix are copied from pageable host memory (the copy
-  // completes before the call returns); the work counter starts at zero.
-  cuda_check(cudaMemcpyAsync(scratch->jobs, dj, n_jobs * sizeof(WalkJobDev), cudaMemcpyHostToDevice, stream_),
-             "no-alloc jobs H2D");
-  cuda_check(cudaMemcpyAsync(scratch->prefix, prefix, (n_jobs + 1) * 4, cudaMemcpyHostToDevice, stream_),
-             "no-alloc prefix H2D");
-  cuda_check(cudaMemsetAsync(&scratch->queue, 0, 4, stream_), "no-alloc counter reset");
+  // Job table, prefix and a zeroed work counter reach the scratch through a
+  // kernel parameter: nothing is read from host memory after this call returns.
+  k_noalloc_stage<<<1, 256, 0, stream_>>>(in, scratch);
+  cuda_check(cudaGetLastError(), "no-alloc job staging");
+  ++launches_;
   const WalkView W = wview();
   k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), tuning_)), kBlock, 0, stream_>>>(
       W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue, tuning_.walk_chunk);

@@ -177,23 +177,27 @@ int bingo_delete_pairs(bingo_handle* h, const uint32_t* u, const uint32_t* v, ui
 int bingo_walk(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode);
 
 /* Allocation-free walks. No counterpart in the reference: this entry point
- * exists for callers that must not allocate GPU memory while they run - for
- * example a serving loop whose HBM is already budgeted to the graph, a caller
- * capturing work into a CUDA graph (allocation calls are not allowed inside a
- * capture), or an application that owns the device memory pool. It runs the
- * same walks as bingo_walk(jobs, n_jobs, BINGO_WALK_BATCHED), with identical
- * results, but takes its scratch (job table, walk offsets and work counter)
- * from a fixed array compiled into the library instead of allocating it, and
- * never calls cudaMalloc or cudaFree.
+ * exists for callers that cannot call cudaMalloc while they run - a serving
+ * loop whose HBM is already budgeted to the graph and its query outputs, or
+ * an application that owns the device memory pool and forbids allocations
+ * outside it. It runs the same walks as
+ * bingo_walk(jobs, n_jobs, BINGO_WALK_BATCHED), with identical results, but
+ * takes its scratch (job table, walk offsets and work counter, 6.4 KB) from a
+ * fixed array compiled into the library instead of allocating it, and calls
+ * neither cudaMalloc nor cudaFree nor any allocating library routine. The job
+ * table reaches that array as a kernel parameter, so nothing is read from the
+ * caller's host memory after the call returns.
  *
  * Limits: at most 64 jobs per call (more returns BINGO_ERR_INVALID_ARGUMENT);
  * every start array must be device memory or NULL and every output device
  * memory (32-byte aligned for walk apps), since host buffers would need
  * staging memory. The scratch array is shared by every call on a device and
- * keeps the last call's contents; calls whose work overlaps on the GPU (two
- * streams, or two handles on one device, at once) race on it, so issue them
- * in order on one stream. The first call on each device looks up the array's
- * device address; make that first call before any stream capture. */
+ * keeps the last call's contents (the work counter is zeroed by each call);
+ * calls whose work overlaps on the GPU (two streams, or two handles on one
+ * device, at once) race on it, so issue them in order on one stream. The
+ * first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. */
 int bingo_walk_noalloc(bingo_handle* h, const bingo_walk_job* jobs, uint32_t n_jobs);
 
 /* ---- Batched programs -------------------------------------------------

@@ -16,6 +16,8 @@ DRIVER = os.path.join(ROOT, "bingo_b200", "bingo_driver")
 
 
 def _run(*args, timeout=300):
+    if not os.path.exists(DRIVER):  # a build output, not part of the source tree
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "bingo_b200"), DRIVER], check=True)
     return subprocess.run([DRIVER, *args], capture_output=True, text=True, timeout=timeout)
 
 

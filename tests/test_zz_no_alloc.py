@@ -1,9 +1,10 @@
-"""bingo_walk_noalloc: walks for callers that cannot allocate GPU memory
-while they run (a serving loop whose HBM is budgeted to the graph, code
-inside a CUDA-graph capture, applications that own the device memory pool).
-The entry point takes its scratch from a fixed array in the library. Checked
-through the C ABI against the allocating entry point, bingo_walk(BATCHED),
-bit for bit, on two calls in a row. This file is collected last."""
+"""bingo_walk_noalloc: walks for callers that cannot call cudaMalloc while
+they run (a serving loop whose HBM is budgeted to the graph and its outputs,
+an application that owns the device memory pool). The entry point takes its
+scratch from a fixed array in the library. Checked through the C ABI against
+the allocating entry point, bingo_walk(BATCHED), bit for bit, on two calls in
+a row, and checked to leave the handle's device memory and the device's free
+memory unchanged. This file is collected last."""
 import ctypes
 
 import numpy as np
@@ -65,12 +66,26 @@ def test_noalloc_walks_match_allocating_entry_point():
         ref = _abi_jobs(specs, "a")
         assert L.bingo_walk(g.handle, ref, len(specs), BATCHED) == 0, L.bingo_last_error(g.handle)
         mine = _abi_jobs(specs, "b")
+        torch.cuda.synchronize()
+        held = _held(g)
+        free0 = torch.cuda.mem_get_info()[0]
         st = L.bingo_walk_noalloc(g.handle, mine, len(specs))
         assert st == 0, L.bingo_last_error(g.handle)
         torch.cuda.synchronize()
+        # The handle holds no more device memory than before the call.
+        assert _held(g) == held, (call, held, _held(g))
+        if call == 1:
+            # After the first call (which may load the kernels it launches),
+            # the device's free memory does not move either.
+            assert torch.cuda.mem_get_info()[0] == free0
         for s in specs:
             assert torch.equal(s["a"], s["b"]), f"call {call} job {s['job_id']}"
             assert (s["b"] != -9).all()
+
+
+def _held(g):
+    st = g.stats()
+    return st["scratch_bytes"], st["arena_bytes"]
 
 
 def test_noalloc_rejects_what_it_cannot_do_without_allocating():
