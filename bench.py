@@ -17,7 +17,6 @@ import argparse
 import gc
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -35,6 +34,16 @@ BATCH_INS, BATCH_DEL = 50_000, 50_000
 GRAPH_SEED = 1234 + 2
 BYTES_PER_STEP = 32  # algorithmic bytes per produced walk step (vertex 8, alias 8, member 4+4, group 4, store 4)
 WORKLOAD = "plain-deepwalk-rmat20"
+
+
+def headline_config(m: int, world: int) -> dict:
+    """The config block both arms print for the DeepWalk workload."""
+    return {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "m": int(m),
+            "weights": "loguniform[1,2^20)", "walks": 1 << SCALE, "walk_len": WALK_LEN,
+            "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}, "form": "plain (one launch per job)",
+            "l2": "inputs larger than L2 (graph state and 320 MB walk output per step)",
+            "clocks": "nvidia-smi samples from warm-up to the end of the e2e timed region",
+            "parallelism": f"replicas x{world}"}
 
 
 def make_workload(steps_total: int, w_hi: int = W_HI):
@@ -60,14 +69,14 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
-def traffic_per_step():
-    """DRAM bytes per produced step of the walk kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "walk_deepwalk_rmat20.md")
-    try:
-        m = re.search(r"dram_bytes_per_step:\s*([0-9.]+)", open(p).read())
-        return float(m.group(1)) if m else None
-    except OSError:
-        return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per produced step
+# of k_walk<DEEPWALK> on this workload, from one ncu capture of one launch:
+# the 4th walk launch of `bench.py --steps 3 --warmup 3` (the first timed
+# step, 31,776,603 produced steps; 3.219 GB read + 0.335 GB written).
+# roofline.traffic scales it to the live run's steps per launch.
+WALK_DRAM_BYTES_PER_STEP = 112.1
+WALK_DRAM_SOURCE = ("ncu capture of one k_walk<DEEPWALK> launch (4th launch, 31,776,603 steps) of "
+                    "bench.py --steps 3 --warmup 3, scaled to this run's steps per launch")
 
 
 class Clocks:
@@ -190,7 +199,8 @@ class CpuRun:
         steps = int((rows >= 0).sum() - len(starts))
         scale = self.n / walks  # extrapolate the walk sample to one walk per vertex
         value = steps * scale / (t_upd + t_walk * scale)
-        return dict(value=value, t_update=t_upd, t_walk=t_walk, walk_steps=steps, walks=walks,
+        return dict(value=value, ms_per_step=(t_upd + t_walk * scale) * 1e3, t_update=t_upd, t_walk=t_walk,
+                    walk_steps=steps, walks=walks,
                     walk_steps_per_s=steps / t_walk, edge_updates_per_s=(len(ins[0]) + len(dels[0])) / t_upd)
 
 
@@ -202,23 +212,28 @@ def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return
+    # Inputs from the generators linked into the oracle library: this arm
+    # never maps the engine library (libbingo.so).
+    from bingo_b200 import gen
+    from oracle import pyoracle as po
+    gen.bind(po.gen_lib())
     n, src, dst, w, batches = make_workload(args.warmup + args.steps)
     walks = min(args.ref_walks, n)
-    vals, last = [], None
+    vals, ms, last = [], [], None
     cpu = CpuRun(n, src, dst, w)
     for i in range(args.warmup + args.steps):
         r = cpu.step(batches[i], walks, seed=100 + i)
         if i >= args.warmup:
             vals.append(r["value"])
+            ms.append(r["ms_per_step"])
             last = r
     value = float(np.mean(vals))
     cores = os.cpu_count()
     line = {
         "impl": "reference", "metric": "walk_steps_per_s", "value": value, "unit": "steps/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "weights": "loguniform[1,2^20)",
-                   "walks": n, "walk_len": WALK_LEN, "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}},
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": headline_config(len(src), world),
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
                          "sample": f"per step: one full 50K+50K update batch + {walks} walks x {WALK_LEN} "
                                    f"(oracle port, {CPU_WALK_FORM})" + scaled_note(walks, n)},
@@ -348,9 +363,14 @@ def run_batched(args):
         return {"walk_steps_per_s": wsteps / (ms / 1e3), "ms_per_step": ms / args.steps,
                 "edge_updates_per_s": upd / (ms / 1e3), "walk_steps_per_step": wsteps / args.steps}
 
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_busy0 = time.time()
     plain = time_form("plain")
     default = time_form("batched-default")
     batched = time_form("batched")
+    clk = clocks.stop(t_busy0, time.time())
     if rank == 0:
         line = {"metric": "walk_steps_per_s", "value": batched["walk_steps_per_s"], "unit": "steps/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched["ms_per_step"],
@@ -363,7 +383,7 @@ def run_batched(args):
                            "form": "one CUDA graph per step: 16 x (16-job persistent walk launch, insert, delete)",
                            "knobs": "autotuned (bingo_autotune) before the timed steps"},
                 "batched": batched, "plain": plain, "batched_default_knobs": default, "autotune": tune_report,
-                "batched_over_plain": batched["walk_steps_per_s"] / plain["walk_steps_per_s"]}
+                "batched_over_plain": batched["walk_steps_per_s"] / plain["walk_steps_per_s"], "clocks": clk}
         print(json.dumps(line), flush=True)
 
 
@@ -464,6 +484,10 @@ def run_served(args):
             g.delete_batch(*x)
 
     results = []
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_busy0 = time.time()
     for ri, (rate, tr) in enumerate(zip(rates, traces)):
         outs = outputs(tr)
         # ---- served: continuous batching
@@ -536,6 +560,7 @@ def run_served(args):
                       "walk_steps_per_s": plain_steps / plain_span, "requests_per_s": len(tr) / plain_span,
                       "span_s": plain_span, "slowest_requests": sorted(((i,) + t for i, t in enumerate(ptrace)), key=lambda z: -z[4])[:8]},
         })
+    clk = clocks.stop(t_busy0, time.time())
     best = max(results, key=lambda r: r["served"]["walk_steps_per_s"])
     line = {"metric": "walk_steps_per_s", "value": best["served"]["walk_steps_per_s"], "unit": "steps/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
@@ -543,7 +568,7 @@ def run_served(args):
                        "weights": "loguniform[1,2^32)", "p_update": args.p_update, "walk_len": WALK_LEN,
                        "requests_per_rate": args.requests, "serve_budget_mb": args.serve_budget,
                        "latency": "arrival (scheduled) to result in pinned host memory"},
-            "sweep": results}
+            "sweep": results, "clocks": clk}
     print(json.dumps(line), flush=True)
 
 
@@ -641,7 +666,12 @@ def run_node2vec(args):
         return
     total = args.warmup + args.steps
     n, src, dst, w, batches = make_node2vec_workload(total)
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_busy0 = time.time()
     r = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=N_LEN, p=0.5, q=2.0)
+    clk = clocks.stop(t_busy0, time.time())
     peak, peak_src = peak_hbm()
     cpu = None
     if not args.no_cpu:
@@ -664,8 +694,90 @@ def run_node2vec(args):
                          "frac": r["algorithmic_gbs"] / peak, "traffic": None, "peak_source": peak_src,
                          "kernel": "k_walk_plain<NODE2VEC>",
                          "bytes": f"{N2V_BYTES_PER_TRIAL} B per proposal + {N2V_BYTES_PER_PROBE} B per probe"},
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "clocks": clk, "store_check": r["store_check"]}
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- the other workloads, one line
+# The default run also measures the node2vec, batched and served workloads
+# and the reference's own CUDA build, each in a child process of its own
+# (fresh device memory, its own clock record), and reports them as keys of
+# the one JSON line.
+EXTRA_RUNS = {
+    "node2vec_cfg3": ["bench.py", "--workload", "node2vec", "--steps", "3", "--warmup", "3", "--no-cpu"],
+    "batched_cfg4": ["bench.py", "--workload", "batched", "--steps", "3", "--warmup", "3"],
+    "served_cfg5": ["bench.py", "--workload", "served", "--rates", "4000,16000", "--requests", "400"],
+    "reference_cuda_cfg2": ["oracle/compare_reference_cuda.py", "--workload", "plain", "--steps", "3",
+                            "--warmup", "3"],
+}
+
+
+def run_child(argv, timeout=900):
+    t0 = time.time()
+    try:
+        r = subprocess.run([sys.executable] + argv, capture_output=True, text=True, timeout=timeout, cwd=ROOT)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode or not lines:
+        return {"error": f"exit {r.returncode}", "stderr_tail": r.stderr[-800:]}
+    d = json.loads(lines[-1])
+    d["wall_s"] = round(time.time() - t0, 1)
+    return d
+
+
+def summarize_extra(key, d):
+    """The figures of a child run's line that the headline line carries."""
+    if "error" in d or "unavailable" in d:
+        return d
+    keep = {"node2vec_cfg3": ("value", "unit", "ms_per_step", "walk_steps_per_s", "edge_updates_per_s", "node2vec",
+                              "roofline", "config", "clocks", "store_check", "wall_s"),
+            "batched_cfg4": ("value", "unit", "ms_per_step", "config", "plain", "batched", "batched_default_knobs",
+                             "batched_over_plain", "clocks", "wall_s"),
+            "served_cfg5": ("value", "unit", "config", "clocks", "wall_s"),
+            "reference_cuda_cfg2": ("config", "reference", "ours_same_input", "clocks", "wall_s")}[key]
+    out = {k: d[k] for k in keep if k in d}
+    if key == "batched_cfg4" and "autotune" in d:
+        out["autotune_knobs"] = {k: v for k, v in d["autotune"].items() if k != "trials"}
+    if key == "served_cfg5":
+        out["sweep"] = []
+        for r in d["sweep"]:
+            row = {k: r[k] for k in ("rate_req_s", "requests", "walk_queries", "update_batches", "update_edges")}
+            for form in ("served", "plain"):
+                row[form] = {k: r[form][k] for k in ("walk_p50_ms", "walk_p99_ms", "update_p50_ms", "update_p99_ms",
+                                                     "walk_steps_per_s", "requests_per_s", "span_s")}
+            row["served_over_plain_req_s"] = r["served"]["requests_per_s"] / r["plain"]["requests_per_s"]
+            out["sweep"].append(row)
+    if key == "reference_cuda_cfg2":
+        ref, ours = d["reference"], d["ours_same_input"]
+        out["ours_over_reference"] = {k: ours[k] / ref[k] for k in ("value", "walk_steps_per_s", "edge_updates_per_s")}
+    return out
+
+
+def run_extras():
+    out = {}
+    for key, argv in EXTRA_RUNS.items():
+        out[key] = summarize_extra(key, run_child(argv))
+    targets = {}
+    b = out.get("batched_cfg4", {})
+    if "batched_over_plain" in b:
+        targets["batched_over_plain_cfg4"] = b["batched_over_plain"]
+    sv = out.get("served_cfg5", {})
+    if sv.get("sweep"):
+        top = max(sv["sweep"], key=lambda r: r["rate_req_s"])
+        targets["served_over_plain_req_s_cfg5"] = top["served_over_plain_req_s"]
+    rc = out.get("reference_cuda_cfg2", {})
+    if "ours_over_reference" in rc:
+        targets["steps_over_reference_cuda_cfg2"] = rc["ours_over_reference"]["value"]
+        targets["walk_kernel_over_reference_cuda_cfg2"] = rc["ours_over_reference"]["walk_steps_per_s"]
+    out["targets"] = targets
+    return out
+
+
+def under_profiler() -> bool:
+    """True inside an Nsight Compute (or other CUDA injection) run: the child
+    workloads are then skipped, so a capture never follows them."""
+    return bool(os.environ.get("CUDA_INJECTION64_PATH") or os.environ.get("NV_COMPUTE_PROFILER_PERFWORKS_DIR"))
 
 
 # --------------------------------------------------------------------------- GPU arm
@@ -816,9 +928,9 @@ def run_ours(args):
     # ---- roofline of the walk kernel
     peak, peak_src = peak_hbm()
     achieved = steps_local * BYTES_PER_STEP / (walk_ms / 1e3) / 1e9
-    tps = traffic_per_step()
+    tps = WALK_DRAM_BYTES_PER_STEP
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": (tps * steps_local / args.steps) if tps else None, "peak_source": peak_src,
+            "traffic": tps * steps_local / args.steps, "traffic_source": WALK_DRAM_SOURCE, "peak_source": peak_src,
             "kernel": "k_walk_plain<DEEPWALK>", "bytes_per_step": BYTES_PER_STEP}
     if tps:
         # DRAM bytes the kernel actually moves per second (ncu bytes per step x
@@ -841,18 +953,18 @@ def run_ours(args):
                          f"oracle ({CPU_WALK_FORM})" + scaled_note(args.cpu_walks, n),
                "walk_steps_per_s": r["walk_steps_per_s"], "edge_updates_per_s": r["edge_updates_per_s"]}
 
+    g.close()
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and not under_profiler():
+        extras = run_extras()
+
     if rank == 0:
         line = {
             "metric": "walk_steps_per_s", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "scale": SCALE, "edge_factor": EDGE_FACTOR, "m": int(len(src)),
-                       "weights": "loguniform[1,2^20)", "walks": n, "walk_len": WALK_LEN,
-                       "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}, "form": "plain (one launch per job)",
-                       "l2": "inputs larger than L2 (graph state and 320 MB walk output per step)",
-                       "clocks": "nvidia-smi samples from warm-up to the end of the e2e timed region",
-                       "parallelism": f"replicas x{world}"},
+            "config": headline_config(len(src), world),
             "walk_steps_per_s": steps_local / (walk_ms / 1e3),
             "edge_updates_per_s": (BATCH_INS + BATCH_DEL) * args.steps / (upd_ms / 1e3),
             "e2e": e2e,
@@ -862,8 +974,9 @@ def run_ours(args):
             "gpu_launches": int(launches) * world,
             "store_check": store_check,
         }
+        if extras is not None:
+            line["other_workloads"] = extras
         print(json.dumps(line), flush=True)
-    g.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -890,6 +1003,8 @@ def main():
     ap.add_argument("--ref-walks", type=int, default=1 << 20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the node2vec / batched / served / reference-CUDA child runs of the default workload")
     ap.add_argument("--no-gather-ceiling", action="store_true",
                     help="skip measuring the GPU's random 32-byte-sector read ceiling (4 GiB table, ~1 s)")
     args = ap.parse_args()

@@ -9,7 +9,29 @@ import os
 
 import numpy as np
 
-from ._lib import lib
+from ._lib import SIGNATURES, lib
+
+_bound = None
+
+
+def bind(cdll) -> None:
+    """Take the generators from another library that exports the same
+    bingo_gen_* / bingo_updgen_* / bingo_edge_list_read / bingo_driver_weights
+    symbols (compiled from the same gen.cpp); None returns to libbingo.so.
+    A CPU-only caller uses this to build workloads without loading the engine."""
+    global _bound
+    if cdll is not None:
+        for name, (res, args) in SIGNATURES.items():
+            if name.startswith(("bingo_gen_", "bingo_updgen_", "bingo_edge_list_", "bingo_driver_weights")):
+                f = getattr(cdll, name)
+                f.restype = res
+                f.argtypes = args
+    _bound = cdll
+
+
+def _lib():
+    return _bound if _bound is not None else lib()
+
 
 W_UNIFORM, W_LOGUNIFORM, W_ZIPF = 0, 1, 2
 DRIVER_AUTO, DRIVER_DEGREE, DRIVER_DEGREE_POW03 = 0, 1, 2
@@ -25,13 +47,13 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
     cap = edge_factor << scale
     src = np.empty(cap, np.uint32)
     dst = np.empty(cap, np.uint32)
-    m = lib().bingo_gen_rmat(scale, edge_factor, a, b, c, seed, _p(src), _p(dst))
+    m = _lib().bingo_gen_rmat(scale, edge_factor, a, b, c, seed, _p(src), _p(dst))
     return src[:m].copy(), dst[:m].copy()
 
 
 def weights(m: int, dist: int = W_UNIFORM, lo: float = 1, hi: float = 1024, s: float = 1.2, seed: int = 2):
     w = np.empty(m, np.uint32)
-    lib().bingo_gen_weights(m, dist, lo, hi, s, seed, _p(w))
+    _lib().bingo_gen_weights(m, dist, lo, hi, s, seed, _p(w))
     return w
 
 
@@ -42,7 +64,7 @@ class UpdateGen:
     def __init__(self, n: int, src: np.ndarray, dst: np.ndarray, seed: int = 3):
         src = np.ascontiguousarray(src, np.uint32)
         dst = np.ascontiguousarray(dst, np.uint32)
-        self._L = lib()
+        self._L = _lib()
         self._g = self._L.bingo_updgen_create(n, _p(src), _p(dst), len(src), seed)
 
     def inserts(self, k: int, dist: int = W_UNIFORM, lo: float = 1, hi: float = 1024, s: float = 1.2):
@@ -72,7 +94,7 @@ def read_edge_list(path: str):
     """An edge-list file as the reference's loadGraph() reads it ("u v" pairs,
     include/graph.cuh:22-27; '#'/'%' comment lines skipped). Returns
     (src, dst, n) with ids as in the file and n = largest id + 1."""
-    L = lib()
+    L = _lib()
     m, n = ctypes.c_uint64(), ctypes.c_uint32()
     bp = os.fsencode(path)
     rc = L.bingo_edge_list_read(bp, None, None, 0, ctypes.byref(m), ctypes.byref(n))
@@ -91,7 +113,7 @@ def driver_weights(src, dst, n: int, kind: int = DRIVER_AUTO):
     bias(d) = d, or d^0.3 for n > 1e7 (include/graph.cuh:43-51, include/api.h:29-30)."""
     s, d = np.ascontiguousarray(src, np.uint32), np.ascontiguousarray(dst, np.uint32)
     w = np.empty(len(s), np.uint32)
-    if lib().bingo_driver_weights(kind, _p(s), _p(d), len(s), n, _p(w)):
+    if _lib().bingo_driver_weights(kind, _p(s), _p(d), len(s), n, _p(w)):
         raise ValueError("unknown weight kind or an id >= n")
     return w
 

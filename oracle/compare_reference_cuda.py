@@ -20,6 +20,7 @@ import json
 import os
 import subprocess
 import sys
+import time
 
 import numpy as np
 
@@ -27,7 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
 from bench import (BATCH_DEL, BATCH_INS, EDGE_FACTOR, N_BATCH, N_SCALE, SCALE, WALK_LEN, WORKLOAD,  # noqa: E402
-                   dist_setup, make_node2vec_workload, make_workload, measure_engine)
+                   Clocks, dist_setup, make_node2vec_workload, make_workload, measure_engine)
 
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
 
@@ -86,7 +87,12 @@ def run_reference_cuda(args):
                 f.write(np.stack(dels, 1).astype("<u4").tobytes())
                 f.write(struct.pack("<IIIQ", 4, 1 if n2v else 0, 1, 1000 + i))
             f.write(struct.pack("<I", 0))
+        clocks = Clocks(local)
+        clocks.start()
+        time.sleep(0.3)
+        t_busy0 = time.time()
         r = subprocess.run([REF_HARNESS, inp, "-"], capture_output=True, text=True, timeout=1800)
+        clk_ref = clocks.stop(t_busy0, time.time())
     if r.returncode:
         print(json.dumps({"impl": "reference-cuda", "unavailable": f"ref_harness exited {r.returncode}: "
                           + r.stderr.strip().splitlines()[-1][:200] if r.stderr.strip() else "no message"}))
@@ -103,6 +109,10 @@ def run_reference_cuda(args):
            "walk_kernel_ms_per_step": walk_s * 1e3 / len(walks),
            "update_wall_ms_per_step": (sum(ins_s) + sum(del_s)) * 1e3 / len(walks),
            "steps_per_walk_phase": steps / len(walks)}
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    t_busy0 = time.time()
     if n2v:
         from bingo_b200 import NODE2VEC
         ours = measure_engine(args, n, src, dst, w, batches, local, app=NODE2VEC, length=WALK_LEN, p=0.5, q=2.0)
@@ -122,9 +132,11 @@ def run_reference_cuda(args):
         cfg = {"workload": WORKLOAD + "-w16", "scale": SCALE, "edge_factor": EDGE_FACTOR,
                "weights": "loguniform[1,2^16)", "walks": n, "walk_len": WALK_LEN,
                "batch": {"insert": BATCH_INS, "delete": BATCH_DEL}}
+    clk_ours = clocks.stop(t_busy0, time.time())
     line = {"impl": "reference-cuda", "metric": "walk_steps_per_s", "value": ref["value"], "unit": "steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "config": cfg, "reference": ref, "ours_same_input": ours}
+            "config": cfg, "reference": ref, "ours_same_input": ours,
+            "clocks": {"reference": clk_ref, "ours": clk_ours}}
     print(json.dumps(line), flush=True)
 
 

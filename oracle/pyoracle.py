@@ -61,6 +61,13 @@ def lib():
     return _L
 
 
+def gen_lib():
+    """This library as a source of the seeded workload generators (the same
+    gen.cpp the engine library compiles, linked into liboracle.so), for
+    callers that must not load the engine (bingo_b200.gen.bind)."""
+    return lib()
+
+
 def _p(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
