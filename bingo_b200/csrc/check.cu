@@ -56,7 +56,8 @@ __device__ __forceinline__ int nth_set_bit(uint32_t x, uint32_t j) {
 }
 
 __device__ __forceinline__ bool group_extent_ok(const GroupDesc& G, unsigned long long top_member) {
-  return G.cnt <= G.cap && (!G.cap || within((unsigned long long)G.base * 4, G.cap, top_member));
+  if (!G.base1) return G.cnt == 0;
+  return G.cnt <= (1u << 31) && within((unsigned long long)group_base(G) * 4, group_cap(G), top_member);
 }
 
 // Lane k of the calling warp holds group k; fills X.
@@ -68,7 +69,7 @@ __device__ __forceinline__ void build_index(GroupIndex& X, const GroupDesc& G, i
     if (lane >= o) incl += y;
   }
   X.off[lane] = incl - G.cnt;
-  X.base[lane] = G.base;
+  X.base[lane] = group_base(G);
   if (lane == 31) X.off[kBits] = incl;
 }
 
@@ -212,13 +213,17 @@ __global__ void __launch_bounds__(kCheckBlock) k_check(StoreView S, CheckTotals*
         const bool mine = (uint32_t)lane < m;
         if (mine) a = S.alias[R.aoff + lane];
         const int own = mine ? nth_set_bit(nz, lane) : 0;
-        const uint32_t own_base = __shfl_sync(kFull, G.base, own), own_cnt = __shfl_sync(kFull, G.cnt, own);
+        // lane k: the (ref, count word) its group is named by in the table
+        // (a one-member group by its member; extents were checked above).
+        const uint32_t gref = G.cnt == 1 ? S.gv[(size_t)group_base(G) * 4] : group_base(G);
+        const uint32_t gcw = G.cnt == 1 ? (kInlineGroup | (uint32_t)lane) : (uint32_t)G.cnt;
+        const uint32_t own_ref = __shfl_sync(kFull, gref, own), own_cw = __shfl_sync(kFull, gcw, own);
         int alt = -1;
         for (int l = 0; l < 32; ++l) {
-          const uint32_t bl = __shfl_sync(kFull, G.base, l), cl = __shfl_sync(kFull, G.cnt, l);
-          if (mine && alt < 0 && ((nz >> l) & 1u) && bl == a.alt_base && cl == a.alt_cnt) alt = l;
+          const uint32_t rl = __shfl_sync(kFull, gref, l), cl = __shfl_sync(kFull, gcw, l);
+          if (mine && alt < 0 && ((nz >> l) & 1u) && rl == a.alt_ref && cl == a.alt_cw) alt = l;
         }
-        if (mine && (a.T != T || a.thr > T || a.own_base != own_base || a.own_cnt != own_cnt || alt < 0))
+        if (mine && (a.T != T || a.thr > T || a.own_ref != own_ref || a.own_cw != own_cw || alt < 0))
           bad |= BINGO_CHECK_ALIAS;
         unsigned __int128 acc = 0;
         for (uint32_t j = 0; j < m; ++j) {

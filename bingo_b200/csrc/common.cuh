@@ -28,13 +28,17 @@ struct __align__(16) VertexRec {
 };
 
 // 32 B = one sector. Slot j of a vertex: draw r in [0, T); r < thr picks the
-// slot's own group, otherwise its alias group. Each group is named by its
-// member list (base in 4-entry units of the member arena, count).
+// slot's own group, otherwise its alias group. Each group is named by a
+// (ref, count word) pair: for a list of two or more members, its base (in
+// 4-entry units of the member arena) and its count; for a group of one
+// member, that member's neighbour id and kInlineGroup | k (k = the group's
+// bit), so a draw that lands there needs no member load.
+constexpr uint32_t kInlineGroup = 0x80000000u;
 struct __align__(32) AliasRec {
   unsigned long long thr;
   unsigned long long T;
-  uint32_t own_base, own_cnt;
-  uint32_t alt_base, alt_cnt;
+  uint32_t own_ref, own_cw;
+  uint32_t alt_ref, alt_cw;
 };
 
 struct __align__(16) HashEntry {
@@ -53,11 +57,17 @@ struct __align__(16) EdgeRec {
   uint32_t v, w, ebp, pad;
 };
 
-struct __align__(16) GroupDesc {
-  uint32_t base;  // member arena offset in 4-entry units
-  uint32_t cnt;   // members
-  uint32_t cap;   // capacity in entries (power of two >= kMinGroupCap) or 0
-  uint32_t pad;
+// 8 B (a vertex's 32 descriptors fill two 128-byte lines). The capacity is
+// not stored exactly: a list holds at least group_cap() entries, the power of
+// two >= max(cnt, kMinGroupCap), doubled when `roomy` is set (the list holds
+// at least twice that, as after deletes from a larger count). An append that
+// would pass group_cap() moves the list; the bit keeps a list whose count
+// dips below a power of two and comes back from moving each time. A list
+// emptied by deletes keeps its storage (base1 != 0, cnt 0).
+struct __align__(8) GroupDesc {
+  uint32_t base1;      // member arena offset in 4-entry units, plus 1; 0 = no list
+  uint32_t cnt : 31;   // members
+  uint32_t roomy : 1;  // the list holds at least 2 x pow2(max(cnt, kMinGroupCap)) entries
 };
 
 struct __align__(16) VertexMeta {
@@ -139,6 +149,18 @@ __host__ __device__ __forceinline__ uint32_t pow2_at_least(uint32_t x, uint32_t 
   while (c < x && c) c <<= 1;  // 0 when x exceeds 2^31
   return c;
 }
+
+// Entries the group's list holds at least (0 when it has no list).
+__host__ __device__ __forceinline__ uint32_t group_cap(const GroupDesc& G) {
+  return G.base1 ? pow2_at_least(G.cnt, kMinGroupCap) << G.roomy : 0u;
+}
+// The roomy bit after the count changed in place (no move) from a list
+// whose group_cap() was cap0.
+__host__ __device__ __forceinline__ uint32_t group_roomy(uint32_t cnt, uint32_t cap0) {
+  return 2ull * pow2_at_least(cnt, kMinGroupCap) <= (unsigned long long)cap0 ? 1u : 0u;
+}
+// Member arena offset of the list in 4-entry units (0 when it has no list).
+__host__ __device__ __forceinline__ uint32_t group_base(const GroupDesc& G) { return G.base1 ? G.base1 - 1u : 0u; }
 
 // Adjacency index hash: MurmurHash3 32-bit finaliser (Appleby, public domain).
 __host__ __device__ __forceinline__ uint32_t mix32(uint32_t h) {

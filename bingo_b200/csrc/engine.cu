@@ -27,7 +27,8 @@ namespace {
 constexpr int kBlock = 256;
 constexpr unsigned long long kUnitBytes[kArenas] = {4, sizeof(EdgeRec), 4, sizeof(AliasRec), sizeof(HashEntry)};
 // Index limits imposed by the 32-bit offsets in the walk-side records.
-constexpr unsigned long long kArenaLimit[kArenas] = {(1ull << 34), ~0ull, ~0ull, (1ull << 32), (1ull << 32)};
+// (member lists are named by their offset in 4-entry units plus one, a 32-bit word)
+constexpr unsigned long long kArenaLimit[kArenas] = {(1ull << 34) - 4, ~0ull, ~0ull, (1ull << 32), (1ull << 32)};
 constexpr unsigned long long kArenaFloor[kArenas] = {1024, 1024, 1024, 256, 1024};
 const char* const kArenaName[kArenas] = {"member", "edge", "back-pointer", "alias", "adjacency"};
 
@@ -95,10 +96,24 @@ __device__ __forceinline__ void seg_bounds(const uint32_t* seg, uint32_t S, uint
   *e = s + 1 < S ? seg[s + 1] : (uint32_t)k;
 }
 
-// Per-segment arena sizes (need is [kArenas][ks], zero past the last segment).
+// Arena sizes one segment needs (units of each arena); one exclusive scan
+// over these rows gives every segment its offsets in all arenas at once.
+struct ArenaNeed {
+  unsigned long long v[kArenas];
+};
+struct AddNeed {
+  __host__ __device__ ArenaNeed operator()(const ArenaNeed& a, const ArenaNeed& b) const {
+    ArenaNeed r;
+#pragma unroll
+    for (int i = 0; i < kArenas; ++i) r.v[i] = a.v[i] + b.v[i];
+    return r;
+  }
+};
+
+// Per-segment arena sizes (need[ks], zero past the last segment).
 __global__ void k_plan(StoreView S, const uint32_t* skey, const uint32_t* sw, const uint32_t* seg,
                        const uint32_t* nseg, unsigned long long k, uint32_t ks, const uint32_t* ctl,
-                       unsigned long long* need) {
+                       ArenaNeed* need) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
   const uint32_t nS = *nseg;
@@ -111,28 +126,31 @@ __global__ void k_plan(StoreView S, const uint32_t* skey, const uint32_t* sw, co
       const uint32_t u = skey[b];
       if (u < S.n) plan_append(S, u, sw + b, e - b, nd);
     }
-    if (lane == 0)
-      for (int a = 0; a < kArenas; ++a) need[(size_t)a * ks + s] = nd[a];
+    if (lane == 0) {
+      ArenaNeed r;
+#pragma unroll
+      for (int a = 0; a < kArenas; ++a) r.v[a] = nd[a];
+      need[s] = r;
+    }
   }
 }
 
-__global__ void k_totals(const unsigned long long* need, const unsigned long long* scan, uint32_t ks,
-                         unsigned long long* tot) {
-  const int a = threadIdx.x;
-  if (a < kArenas) tot[a] = ks ? scan[(size_t)a * ks + ks - 1] + need[(size_t)a * ks + ks - 1] : 0;
-}
-
-// All-or-nothing reservation of the batch's arena space.
-// Publishes the insert plan to mapped host memory: out[0..5) totals,
-// out[5] the batch status word, out[6..11) the arena tops.
-__global__ void k_publish_plan(const unsigned long long* tot, const uint32_t* ctl, const unsigned long long* top,
-                               volatile unsigned long long* out) {
+// Batch totals per arena from the scanned needs. With `out` (mapped host
+// memory) it also publishes the insert plan: out[0..5) totals, out[5] the
+// batch status word, out[6..11) the arena tops.
+__global__ void k_totals(const ArenaNeed* need, const ArenaNeed* scan, uint32_t ks, unsigned long long* tot,
+                         const uint32_t* ctl, const unsigned long long* top, volatile unsigned long long* out) {
   const int t = threadIdx.x;
-  if (t < kArenas) out[t] = tot[t];
+  const unsigned long long x = t < kArenas && ks ? scan[ks - 1].v[t] + need[ks - 1].v[t] : 0ull;
+  if (t < kArenas) tot[t] = x;
+  if (!out) return;
+  if (t < kArenas) out[t] = x;
   if (t == kArenas) out[kArenas] = *ctl;
   if (t < kArenas) out[kArenas + 1 + t] = top[t];
   __threadfence_system();
 }
+
+// All-or-nothing reservation of the batch's arena space.
 
 __global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base) {
   if (threadIdx.x || blockIdx.x || *ctl) return;
@@ -154,7 +172,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint
                                                          const uint32_t* sw, const uint32_t* sorig,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, uint32_t ks, const uint32_t* ctl,
-                                                         const unsigned long long* scan,
+                                                         const ArenaNeed* scan,
                                                          const unsigned long long* base, uint32_t* out_slots) {
   if (*ctl) return;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
@@ -164,9 +182,10 @@ __global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint
     seg_bounds(seg, nS, s, k, &b, &e);
     const uint32_t u = skey[b];
     if (u >= S.n) continue;
+    const ArenaNeed off = scan[s];
     unsigned long long res[kArenas];
 #pragma unroll
-    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + scan[(size_t)a * ks + s];
+    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + off.v[a];
     apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res);
   }
 }
@@ -665,8 +684,8 @@ void Engine::ensure_batch_scratch(uint64_t k) {
   nseg_.ensure(16, "scratch");
   ctl_.ensure(16, "scratch");
   base_.ensure(kArenas * 8 * 2, "scratch");
-  need_.ensure((size_t)kArenas * ks * 8, "scratch");
-  scan_.ensure((size_t)kArenas * ks * 8, "scratch");
+  need_.ensure((size_t)ks * sizeof(ArenaNeed), "scratch");
+  scan_.ensure((size_t)ks * sizeof(ArenaNeed), "scratch");
   if (iota_n_ < kk) {
     iota_.ensure(kk * 4, "scratch");
     k_iota<<<grid_for(kk, kBlock), kBlock, 0, stream_>>>(iota_.as<uint32_t>(), kk);
@@ -679,8 +698,8 @@ void Engine::ensure_batch_scratch(uint64_t k) {
                                   (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)kk, 0, 32, stream_);
   cub::DeviceSelect::Flagged(nullptr, t_sel, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
                              (uint32_t*)nullptr, (int)kk, stream_);
-  cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                (int)ks, stream_);
+  cub::DeviceScan::ExclusiveScan(nullptr, t_scan, (const ArenaNeed*)nullptr, (ArenaNeed*)nullptr, AddNeed(),
+                                 ArenaNeed{}, (int)ks, stream_);
   cub_tmp_.ensure(std::max(t_sort, std::max(t_sel, t_scan)), "scratch");
 }
 
@@ -779,29 +798,34 @@ void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
   ++arena_gen_;
 }
 
+// Per-segment arena needs of the grouped insert batch, their exclusive scan
+// (each segment's offsets in every arena) and the batch totals, which it
+// returns (device memory); publish != null also writes the insert plan there.
+unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t ks,
+                                       volatile unsigned long long* publish) {
+  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
+      S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
+      ctl_.as<uint32_t>(), need_.as<ArenaNeed>());
+  cuda_check(cudaGetLastError(), "plan");
+  ++launches_;
+  size_t tb = cub_tmp_.bytes;
+  cuda_check(cub::DeviceScan::ExclusiveScan(cub_tmp_.p, tb, need_.as<ArenaNeed>(), scan_.as<ArenaNeed>(), AddNeed(),
+                                            ArenaNeed{}, (int)ks, stream_),
+             "scan");
+  unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
+  k_totals<<<1, 32, 0, stream_>>>(need_.as<ArenaNeed>(), scan_.as<ArenaNeed>(), ks, d_tot, ctl_.as<uint32_t>(),
+                                  d_top_, publish);
+  cuda_check(cudaGetLastError(), "totals");
+  ++launches_;
+  return d_tot;
+}
+
 // Plan, size, reserve and apply an append batch whose grouped columns are in
 // key_s_/sa_ (dst)/sb_ (w)/perm_ (original index) and segments in seg_/nseg_.
 void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t) {
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   const StoreView S0 = view();
-  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
-      S0, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
-      ctl_.as<uint32_t>(), need_.as<unsigned long long>());
-  cuda_check(cudaGetLastError(), "plan");
-  ++launches_;
-  for (int a = 0; a < kArenas; ++a) {
-    size_t tb = cub_tmp_.bytes;
-    cuda_check(cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tb, need_.as<unsigned long long>() + (size_t)a * ks,
-                                             scan_.as<unsigned long long>() + (size_t)a * ks, (int)ks, stream_),
-               "scan");
-  }
-  unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
-  k_totals<<<1, 32, 0, stream_>>>(need_.as<unsigned long long>(), scan_.as<unsigned long long>(), ks, d_tot);
-  cuda_check(cudaGetLastError(), "totals");
-  ++launches_;
-  k_publish_plan<<<1, 32, 0, stream_>>>(d_tot, ctl_.as<uint32_t>(), d_top_, d_plan_);
-  cuda_check(cudaGetLastError(), "publish plan");
-  ++launches_;
+  unsigned long long* d_tot = plan_needs(S0, k, ks, d_plan_);
   cuda_check(cudaStreamSynchronize(stream_), "plan sync");
   unsigned long long tot[kArenas];
   for (int a = 0; a < kArenas; ++a) tot[a] = h_plan_[a];
@@ -825,7 +849,7 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   ++launches_;
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
       base_.as<unsigned long long>(), dev_out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
@@ -1336,27 +1360,13 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   ++launches_;
   group_by_vertex(a, b, c, k);
   const StoreView S = view();
-  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
-      S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
-      ctl_.as<uint32_t>(), need_.as<unsigned long long>());
-  cuda_check(cudaGetLastError(), "plan");
-  ++launches_;
-  for (int ar = 0; ar < kArenas; ++ar) {
-    size_t tb = cub_tmp_.bytes;
-    cuda_check(cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tb, need_.as<unsigned long long>() + (size_t)ar * ks,
-                                             scan_.as<unsigned long long>() + (size_t)ar * ks, (int)ks, stream_),
-               "scan");
-  }
-  unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
-  k_totals<<<1, 32, 0, stream_>>>(need_.as<unsigned long long>(), scan_.as<unsigned long long>(), ks, d_tot);
-  cuda_check(cudaGetLastError(), "totals");
-  ++launches_;
+  unsigned long long* d_tot = plan_needs(S, k, ks, nullptr);
   k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
   cuda_check(cudaGetLastError(), "reserve");
   ++launches_;
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<unsigned long long>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
       base_.as<unsigned long long>(), out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
@@ -1803,7 +1813,7 @@ void Engine::dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, ui
       const GroupDesc& G = H.gd[(size_t)u * kBits + k];
       gcnt[(size_t)u * kBits + k] = G.cnt;
       for (uint32_t p = 0; p < G.cnt; ++p, ++mem) {
-        const size_t idx = (size_t)G.base * 4 + p;
+        const size_t idx = (size_t)group_base(G) * 4 + p;
         const uint32_t sl = H.gs[idx];
         mslot[mem] = sl;
         mv[mem] = H.gv[idx];
@@ -1822,9 +1832,13 @@ void Engine::dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, ui
       aT[a] = A.T;
       aown[a] = j < (uint32_t)nnz ? (uint8_t)nzbits[j] : 255;
       uint8_t alt = 255;
-      for (int k = 0; k < kBits; ++k) {
-        const GroupDesc& G = H.gd[(size_t)u * kBits + k];
-        if (G.cnt && G.base == A.alt_base && G.cnt == A.alt_cnt) alt = (uint8_t)k;
+      if (A.alt_cw & kInlineGroup) {
+        alt = (uint8_t)(A.alt_cw & (kBits - 1));  // a one-member group names its bit
+      } else {
+        for (int k = 0; k < kBits; ++k) {
+          const GroupDesc& G = H.gd[(size_t)u * kBits + k];
+          if (G.cnt > 1 && group_base(G) == A.alt_ref && G.cnt == A.alt_cw) alt = (uint8_t)k;
+        }
       }
       aalias[a] = alt;
     }
@@ -1927,7 +1941,7 @@ struct SnapHeader {
   uint64_t checksum;
 };
 constexpr char kSnapMagic[8] = {'B', 'I', 'N', 'G', 'O', 'S', 'N', 'P'};
-constexpr uint32_t kSnapVersion = 1;
+constexpr uint32_t kSnapVersion = 2;  // 2: 8-byte group descriptors, one-member groups named inline in the alias table
 constexpr size_t kSnapChunk = 64u << 20;
 
 // Word-wise multiply-xor hash (64-bit lanes, tail bytes folded in one by one).

@@ -172,6 +172,7 @@ class Engine {
   const uint32_t* stage(const uint32_t* p, uint64_t k, DevBuf& buf, const char* what);
   void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k);
   void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
+  unsigned long long* plan_needs(const StoreView& S, uint64_t k, uint32_t ks, volatile unsigned long long* publish);
   void enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k, uint32_t* out_slots);
   void enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k);
   void ensure_headroom(uint64_t k_insert_total);

@@ -15,7 +15,11 @@ namespace bingo {
 // the total come from ballots and shuffles; the pairing loop runs at most
 // m - 1 times. Replaces the single-lane float construction of
 // include/Bingo.cuh:111-158.
-__device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uint32_t base, AliasRec* out) {
+//
+// single: the member of this lane's group when cnt == 1 (the table names a
+// one-member group by its member, AliasRec).
+__device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uint32_t base, uint32_t single,
+                                                     AliasRec* out) {
   const unsigned long long mass = (unsigned long long)cnt << lane;
   const uint32_t nz = __ballot_sync(kFull, cnt != 0);
   const uint32_t m = __popc(nz);
@@ -64,17 +68,20 @@ __device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uin
     }
   }
   // Remaining groups hold exactly T: thr = T, alias = self (already set).
-  const uint32_t alt_base = __shfl_sync(kFull, base, alias_lane);
-  const uint32_t alt_cnt = __shfl_sync(kFull, cnt, alias_lane);
+  // A one-member group is named by its member (AliasRec).
+  const uint32_t ref = cnt == 1 ? single : base;
+  const uint32_t cw = cnt == 1 ? (kInlineGroup | (uint32_t)lane) : cnt;
+  const uint32_t alt_ref = __shfl_sync(kFull, ref, alias_lane);
+  const uint32_t alt_cw = __shfl_sync(kFull, cw, alias_lane);
   if (cnt) {
     const uint32_t j = __popc(nz & lanemask_lt());
     AliasRec r;
     r.thr = thr;
     r.T = T;
-    r.own_base = base;
-    r.own_cnt = cnt;
-    r.alt_base = alt_base;
-    r.alt_cnt = alt_cnt;
+    r.own_ref = ref;
+    r.own_cw = cw;
+    r.alt_ref = alt_ref;
+    r.alt_cw = alt_cw;
     out[j] = r;
   }
   return m;
@@ -157,7 +164,7 @@ __device__ __forceinline__ GrowPlan plan_growth(int lane, const VertexMeta& M, c
   const uint32_t bpn = M.bpcnt + pc_total;
   p.new_bpcap = bpn > M.bpcap ? pow2_at_least(bpn, kMinEdgeCap) : 0;
   const uint32_t cnt = G.cnt + add_lane;
-  p.gcap_lane = cnt > G.cap ? pow2_at_least(cnt, kMinGroupCap) : 0;
+  p.gcap_lane = cnt > group_cap(G) ? pow2_at_least(cnt, kMinGroupCap) : 0;
   const uint32_t incl = warp_incl_scan(p.gcap_lane, lane);
   p.gsum = __shfl_sync(kFull, incl, 31);
   p.gpre = incl - p.gcap_lane;
@@ -216,9 +223,15 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
   const int lane = threadIdx.x & 31;
   VertexMeta M = S.meta[u];
   GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
+  const uint32_t cap0 = group_cap(G);
   uint32_t add_lane, pc_total;
   count_bits(lane, seg_w, len, &add_lane, &pc_total);
   const GrowPlan P = plan_growth(lane, M, G, len, add_lane, pc_total, S.node2vec);
+  // Loaded here, before any store of this warp: the vertex record, and the
+  // member of a one-member group the batch leaves alone (the alias table
+  // names such a group by its member).
+  VertexRec R = S.vrec[u];
+  uint32_t single = G.cnt == 1 && add_lane == 0 ? S.gv[(size_t)group_base(G) * 4] : 0u;
 
   // --- relocations (old contents keep their order) ---
   if (P.new_ecap) {
@@ -238,17 +251,16 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
     while (grow) {
       const int k = __ffs(grow) - 1;
       grow &= grow - 1;
-      const uint32_t ob = __shfl_sync(kFull, G.base, k), oc = __shfl_sync(kFull, G.cnt, k);
+      const uint32_t ob = __shfl_sync(kFull, group_base(G), k), oc = __shfl_sync(kFull, G.cnt, k);
       const unsigned long long nb = res[A_MEMBER] + __shfl_sync(kFull, P.gpre, k);  // entries
       warp_copy_u32(S.gv + nb, S.gv + (size_t)ob * 4, oc, lane);
       warp_copy_u32(S.gs + nb, S.gs + (size_t)ob * 4, oc, lane);
       if (lane == k) {
-        G.base = (uint32_t)(nb >> 2);
-        G.cap = P.gcap_lane;
+        G.base1 = (uint32_t)(nb >> 2) + 1u;
+        G.roomy = 0;
       }
     }
   }
-  VertexRec R = S.vrec[u];
   if (P.new_acap) {
     R.aoff = (uint32_t)res[A_ALIAS];
     M.acap = P.new_acap;
@@ -267,10 +279,11 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
     }
     if ((w >> lane) & 1u) {
       const uint32_t pos = G.cnt;
-      const size_t e = (size_t)G.base * 4 + pos;
+      const size_t e = (size_t)group_base(G) * 4 + pos;
       S.gv[e] = v;
       S.gs[e] = slot;
       S.bp[M.bpoff + bpbase + __popc(w & ((1u << lane) - 1u))] = pos;
+      if (pos == 0) single = v;
       ++G.cnt;
     }
     bpbase += __popc(w);
@@ -294,7 +307,7 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
       present &= present - 1;
       const bool has = (w >> k) & 1u;
       const uint32_t b = __ballot_sync(kFull, has);
-      const uint32_t kcnt = __shfl_sync(kFull, G.cnt, k), kbase = __shfl_sync(kFull, G.base, k);
+      const uint32_t kcnt = __shfl_sync(kFull, G.cnt, k), kbase = __shfl_sync(kFull, group_base(G), k);
       if (has) {
         const uint32_t pos = kcnt + __popc(b & lanemask_lt());
         const size_t e = (size_t)kbase * 4 + pos;
@@ -302,7 +315,11 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
         S.gs[e] = slot;
         S.bp[M.bpoff + ebp + __popc(w & ((1u << k) - 1u))] = pos;
       }
-      if (lane == k) G.cnt += __popc(b);
+      const uint32_t first_v = __shfl_sync(kFull, v, __ffs(b) - 1);  // b != 0: bit k is present
+      if (lane == k) {
+        if (kcnt == 0) single = first_v;
+        G.cnt += __popc(b);
+      }
     }
   }
   M.ecnt += len;
@@ -334,8 +351,9 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
   __syncwarp();
 
   // --- alias table over the new counts ---
-  R.m = warp_build_alias(lane, G.cnt, G.base, S.alias + R.aoff);
-  S.gdesc[(size_t)u * kBits + lane] = G;
+  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff);
+  if (add_lane && !P.gcap_lane) G.roomy = group_roomy(G.cnt, cap0);
+  if (add_lane || P.gcap_lane) S.gdesc[(size_t)u * kBits + lane] = G;  // only the descriptors that changed
   if (lane == 0) {
     S.meta[u] = M;
     S.vrec[u] = R;
@@ -378,8 +396,11 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
   VertexMeta M = S.meta[u];
   GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
   VertexRec R = S.vrec[u];
-  const size_t gb = (size_t)G.base * 4;
+  const size_t gb = (size_t)group_base(G) * 4;
+  const uint32_t cnt0 = G.cnt, cap0 = group_cap(G);
   uint32_t rejected = 0;
+  bool front_known = false;  // this lane moved a member into position 0
+  uint32_t front = 0;
   for (uint32_t c = 0; c < len; c += 32) {
     const uint32_t i = c + lane;
     const uint32_t slot = i < len ? seg_slot[i] : 0xffffffffu;
@@ -408,6 +429,7 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
       const uint32_t mv = S.gv[gb + last];
       S.gv[gb + pos] = mv;
       S.gs[gb + pos] = ms;
+      if (pos == 0) front_known = true, front = mv;
       const EdgeRec em = S.edges[M.eoff + ms];
       S.bp[M.bpoff + em.ebp + __popc(em.w & below)] = pos;
       G.cnt = last;
@@ -424,8 +446,13 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
     atomicAdd(&S.err[1], rejected);
     set_err(S.err, E_INVALID_SLOT);
   }
-  R.m = warp_build_alias(lane, G.cnt, G.base, S.alias + R.aoff);
-  S.gdesc[(size_t)u * kBits + lane] = G;
+  // A group left with one member is named by it in the alias table.
+  const uint32_t single = G.cnt == 1 ? (front_known ? front : S.gv[gb]) : 0u;
+  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff);
+  if (G.cnt != cnt0) {  // only the descriptors that changed
+    G.roomy = group_roomy(G.cnt, cap0);
+    S.gdesc[(size_t)u * kBits + lane] = G;
+  }
   if (lane == 0) {
     S.meta[u] = M;
     S.vrec[u] = R;

@@ -2,10 +2,12 @@
 // (include/Bingo.cuh:220-267) and the loops of deepwalkKernel, node2vecKernel,
 // pprKernel and samplingKernel (include/operation.cuh:252-368, :407-430).
 //
-// One step is three dependent loads: the 16 B VertexRec of the current
-// vertex, the 32 B AliasRec of the drawn slot (which carries both candidate
-// groups' member-list base and count), and the 4 B member id. All three go
-// through the read-only path: the store does not change during a walk phase.
+// One step is at most three dependent loads: the 16 B VertexRec of the
+// current vertex, the 32 B AliasRec of the drawn slot (which names both
+// candidate groups: member-list base and count, or for a one-member group the
+// member itself), and the 4 B member id (skipped for a one-member group). All
+// go through the read-only path: the store does not change during a walk
+// phase.
 #pragma once
 #include "common.cuh"
 #include "store.cuh"
@@ -60,18 +62,20 @@ __device__ __forceinline__ VertexRec load_vrec(const WalkView& W, uint32_t u) {
 }
 
 // Weighted neighbour draw at a vertex with R.m > 0: slot = mulhi(x, m),
-// r = mulhi64(y:z, T), group = r < thr ? own : alias, member = mulhi(w, cnt).
+// r = mulhi64(y:z, T), group = r < thr ? own : alias, member = mulhi(w, cnt)
+// (a one-member group carries its member in the slot: mulhi(w, 1) = 0).
 __device__ __forceinline__ uint32_t sample_at(const WalkView& W, const VertexRec& R, const Rand4& r) {
   // The whole 32-byte slot in one 256-bit read-only load (one L1 / L2
   // request instead of two 16-byte ones; slots are 32-byte aligned and no
   // kernel writes the store while walks run).
   const AliasRec* a = W.alias + R.aoff + mulhi32(r.x, R.m);
-  unsigned long long thr, T, own_bc, alt_bc;
-  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(thr), "=l"(T), "=l"(own_bc), "=l"(alt_bc) : "l"(a));
+  unsigned long long thr, T, own_rc, alt_rc;
+  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(thr), "=l"(T), "=l"(own_rc), "=l"(alt_rc) : "l"(a));
   const unsigned long long d = mulhi64(((unsigned long long)r.y << 32) | r.z, T);
-  const unsigned long long bc = d < thr ? own_bc : alt_bc;  // base | cnt << 32
-  const uint32_t base = (uint32_t)bc, cnt = (uint32_t)(bc >> 32);
-  return __ldg(W.gv + (size_t)base * 4 + mulhi32(r.w, cnt));
+  const unsigned long long rc = d < thr ? own_rc : alt_rc;  // ref | count word << 32
+  const uint32_t ref = (uint32_t)rc, cw = (uint32_t)(rc >> 32);
+  if (cw & kInlineGroup) return ref;  // one member, carried in the slot
+  return __ldg(W.gv + (size_t)ref * 4 + mulhi32(r.w, cw));
 }
 
 
