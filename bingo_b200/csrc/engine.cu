@@ -658,7 +658,7 @@ int Engine::sync() {
 }
 
 void Engine::finish_call() {
-  if (!cfg_.synchronous) return;
+  if (!cfg_.synchronous || defer_sync_) return;
   const int st = sync();
   if (st) throw Error(st, last_error);
 }

@@ -111,6 +111,10 @@ class Engine {
   WalkJobDev make_job(const bingo_walk_job& J) const;
   void check_walk_job(const bingo_walk_job& J) const;
   void prepare_batches(uint64_t k) { ensure_batch_scratch(k); }
+  // The serving scheduler enqueues update batches without a host wait per
+  // call (it polls an event instead); device-reported errors then surface
+  // through sync().
+  void set_defer_sync(bool on) { defer_sync_ = on; }
   void count_launch() { ++launches_; }
   uint32_t n() const { return n_; }
   int device() const { return cfg_.device; }
@@ -119,6 +123,7 @@ class Engine {
   bingo_config cfg_;
   cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
   bool loaded_ = false;
+  bool defer_sync_ = false;
   uint32_t n_ = 0;
 
   // store

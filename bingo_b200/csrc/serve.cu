@@ -20,9 +20,12 @@
 // writes the job's sequence number + 1 to a completion word in mapped memory.
 //
 // Host side: a scheduler thread admits queries in submission order (HBM
-// budget for outputs and starts, ring capacity), applies updates after the
-// walks before them have finished, copies finished outputs to the caller's
-// buffers and records submit-to-ready latency.
+// budget for outputs and starts, ring capacity), commits updates once the
+// walks before them have finished on the device, copies finished outputs to
+// the caller's buffers and records submit-to-ready latency. An update batch
+// is enqueued on the engine's stream without a host wait; an event marks its
+// end, the next walk-kernel launch waits for that event on the device, and
+// the update's ticket completes when the scheduler sees the event.
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -225,6 +228,7 @@ Server::Server(Engine& eng, const bingo_serve_config& cfg) : eng_(eng), cfg_(cfg
   cuda_check(cudaMemset(state_.p, 0, sizeof(ServeDevState)), "serve state");
   budget_.ensure(cfg_.output_budget_bytes, "serve output budget");
   eng_.prepare_batches(cfg_.max_update_batch);
+  cuda_check(cudaEventCreateWithFlags(&upd_ev_, cudaEventDisableTiming), "serve update event");
   thread_ = std::thread([this] { loop(); });
 }
 
@@ -238,6 +242,9 @@ Server::~Server() {
   cudaStreamSynchronize(kstream_);
   cudaStreamSynchronize(cstream_);
   cudaStreamSynchronize(rstream_);
+  cudaStreamSynchronize(eng_.stream());
+  eng_.set_defer_sync(false);
+  if (upd_ev_) cudaEventDestroy(upd_ev_);
   for (auto& f : inflight_)
     if (f.ev) cudaEventDestroy(f.ev);
   for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
@@ -405,6 +412,8 @@ void Server::launch_kernel() {
     cudaGetLastError();
     per_sm = 2;
   }
+  // Walks read the graph only after the last update batch has applied.
+  if (upd_recorded_) cuda_check(cudaStreamWaitEvent(kstream_, upd_ev_, 0), "serve launch after update");
   cuda_check(cudaMemsetAsync(&state_.as<ServeDevState>()->closing, 0, 4, kstream_), "serve launch");
   k_serve<<<sms * per_sm, kServeBlock, 0, kstream_>>>(eng_.walk_view(), jobs_.as<WalkJobDev>(), d_ctl_,
                                                        state_.as<ServeDevState>(), d_done_seq_,
@@ -456,6 +465,24 @@ bool Server::step() {
       progress = true;
     } else {
       ++it;
+    }
+  }
+  if (upd_pending_) {
+    const cudaError_t q = cudaEventQuery(upd_ev_);
+    if (q == cudaSuccess) {
+      // Device-reported problems of the batch (skipped deletes) read here;
+      // nothing else runs on the engine's stream meanwhile.
+      const int dev_st = eng_.sync();
+      const int st = upd_status_ ? upd_status_ : dev_st;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        m_.update_ns += now_ns() - upd_t0_;
+      }
+      upd_pending_ = false;
+      finish_ticket(upd_ticket_, st, upd_version_);
+      progress = true;
+    } else if (q != cudaErrorNotReady) {
+      throw Error(BINGO_ERR_CUDA, std::string("serving update: ") + cudaGetErrorString(q));
     }
   }
   const uint64_t t_completed = now_ns();
@@ -528,20 +555,27 @@ bool Server::step() {
         m_.max_inflight = std::max<uint64_t>(m_.max_inflight, inflight_.size());
       }
     } else {
-      // An update waits for every walk admitted before it, then commits.
+      // An update waits until every walk admitted before it has finished on
+      // the device (their result copies may still run: they read query
+      // outputs, not the graph) and the previous update's ticket is done,
+      // then is enqueued on the engine's stream; walks admitted after it
+      // launch behind its event.
       if (!ctl_.drain) {
         ctl_.drain = 1;
         push_ctl();
         drain_since_ = now_ns();
         drain_retired_ = 0;
       }
-      if (!inflight_.empty() || oldest_ != published_jobs_) break;
+      bool walks_done = true;
+      for (const auto& f : inflight_) walks_done = walks_done && f.copying;
+      if (!walks_done || upd_pending_) break;
       if (!drain_retired_) drain_retired_ = now_ns();
       if (kernel_running()) break;
       const uint64_t t_upd = now_ns();
       const NvtxRange nvtx_("bingo serve update");
       int st = BINGO_OK;
       const uint64_t k = r->a.size();
+      eng_.set_defer_sync(true);
       for (uint64_t o = 0; o < k; o += cfg_.max_update_batch) {
         const uint64_t len = std::min<uint64_t>(cfg_.max_update_batch, k - o);
         try {
@@ -559,21 +593,23 @@ bool Server::step() {
           if (st != BINGO_ERR_INVALID_SLOT) break;
         }
       }
+      eng_.set_defer_sync(false);
+      cuda_check(cudaEventRecord(upd_ev_, eng_.stream()), "serve update event");
+      upd_recorded_ = true;
       ++version_;
+      upd_pending_ = true;
+      upd_ticket_ = r->ticket;
+      upd_version_ = version_;
+      upd_status_ = st;
+      upd_t0_ = t_upd;
       ctl_.drain = 0;
       push_ctl();
       {
         std::lock_guard<std::mutex> lk(mu_);
-        m_.update_ns += now_ns() - t_upd;
         m_.drain_wait_ns += t_upd - drain_since_;
         m_.drain_inflight_ns += drain_retired_ - drain_since_;
-      }
-      const uint64_t t = r->ticket;
-      {
-        std::lock_guard<std::mutex> lk(mu_);
         queue_.pop_front();
       }
-      finish_ticket(t, st, version_);
       progress = true;
     }
   }
@@ -611,11 +647,17 @@ void Server::loop() {
         t.done = 1, t.status = e.status, t.done_ns = now_ns();
       }
       inflight_.clear();
+      if (upd_pending_) {
+        Ticket& t = tickets_[upd_ticket_];
+        t.done = 1, t.status = e.status, t.done_ns = now_ns();
+        upd_pending_ = false;
+      }
+      eng_.set_defer_sync(false);
       cv_done_.notify_all();
       quit_ = true;
     }
     std::unique_lock<std::mutex> lk(mu_);
-    const bool idle = queue_.empty() && inflight_.empty();
+    const bool idle = queue_.empty() && inflight_.empty() && !upd_pending_;
     if (quit_ && idle) break;
     if (progress) {
       quiet = 0;

@@ -98,6 +98,14 @@ class Server {
   uint64_t version_ = 0;
   bingo_serve_metrics m_{};  // scheduler counters (guarded by mu_ when read)
   uint64_t drain_since_ = 0, drain_retired_ = 0;
+  // The update batch enqueued on the engine's stream and not yet seen
+  // complete (at most one; upd_ev_ marks its end, and every later walk
+  // launch waits for it on the device).
+  bool upd_pending_ = false;
+  uint64_t upd_ticket_ = 0, upd_version_ = 0, upd_t0_ = 0;
+  int upd_status_ = 0;
+  cudaEvent_t upd_ev_ = nullptr;
+  bool upd_recorded_ = false;
 
   // shared with submitters
   std::mutex mu_;
