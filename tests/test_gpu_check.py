@@ -136,8 +136,16 @@ class Snap:
     def meta(self, u):  # eoff, bpoff, ecnt, ecap, bpcnt, bpcap, live, acap, hkeys, hcap
         return struct.unpack_from("<QQ8I", self.parts[1], u * self.rec[1])
 
-    def group(self, u, k):  # base (4-entry units), cnt, cap
-        return struct.unpack_from("<3I", self.parts[2], (u * 32 + k) * self.rec[2])
+    def group(self, u, k):  # base (4-entry units), cnt, capacity (derived, as the engine derives it)
+        base1, word = struct.unpack_from("<2I", self.parts[2], (u * 32 + k) * self.rec[2])
+        cnt, roomy = word & 0x7FFFFFFF, word >> 31
+        cap = 0
+        if base1:
+            cap = 4
+            while cap < cnt:
+                cap <<= 1
+            cap <<= roomy
+        return (base1 - 1 if base1 else 0), cnt, cap
 
     def edge(self, i):  # v, w, ebp
         return struct.unpack_from("<3I", self.parts[4], i * 16)
@@ -273,7 +281,7 @@ def test_extent_damage(saved, tmp_path):
     # a group list that reaches past the used part of the member arena
     s = Snap(path.read_bytes())
     u = _vertex(s, lambda x: s.group(x, 0)[2] > 0)
-    s.set_u32("gdesc", u * 32 * s.rec[2], s.top[0] // 4)
+    s.set_u32("gdesc", u * 32 * s.rec[2], s.top[0] // 4 + 1)  # list base = the end of the used part
     bad = tmp_path / "extent3.snap"
     s.write(bad)
     _refused(node2vec, path, bad, ex, u, EXTENT)
