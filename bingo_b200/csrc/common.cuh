@@ -144,10 +144,16 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
   return x;
 }
 
+// The smallest power of two >= max(x, lo) (lo a power of two); 0 when x
+// exceeds 2^31.
 __host__ __device__ __forceinline__ uint32_t pow2_at_least(uint32_t x, uint32_t lo) {
-  uint32_t c = lo;
-  while (c < x && c) c <<= 1;  // 0 when x exceeds 2^31
-  return c;
+  if (x <= lo) return lo;
+  if (x > 0x80000000u) return 0u;
+#ifdef __CUDA_ARCH__
+  return 1u << (32 - __clz(x - 1));
+#else
+  return 1u << (32 - __builtin_clz(x - 1));
+#endif
 }
 
 // Entries the group's list holds at least (0 when it has no list).

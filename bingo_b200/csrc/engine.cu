@@ -168,7 +168,7 @@ __global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* 
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint32_t* skey, const uint32_t* sv,
+__global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const uint32_t* skey, const uint32_t* sv,
                                                          const uint32_t* sw, const uint32_t* sorig,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, uint32_t ks, const uint32_t* ctl,
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_insert(StoreView S, const uint
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
+__global__ void __launch_bounds__(kBlock, 4) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, const uint32_t* ctl) {
   __shared__ uint32_t stage[kBlock / 32][64];

@@ -202,9 +202,27 @@ __device__ __forceinline__ void count_bits(int lane, const uint32_t* seg_w, uint
   *pc_total = warp_sum_u32(pc);
 }
 
-// Warp copy of n 32-bit words.
+// Warp copy of n 16-byte units between non-overlapping ranges, two 16-byte
+// loads per lane in flight (a relocation of thousands of entries costs tens
+// of round trips, not one per 32 entries; four in flight pushed the insert
+// kernel past 64 registers).
+__device__ __forceinline__ void warp_copy_v4(uint4* __restrict__ dst, const uint4* __restrict__ src, uint32_t n,
+                                             int lane) {
+  uint32_t i = lane;
+  for (; i + 32 < n; i += 64) {
+    const uint4 a = src[i], b = src[i + 32];
+    dst[i] = a;
+    dst[i + 32] = b;
+  }
+  for (; i < n; i += 32) dst[i] = src[i];
+}
+
+// Warp copy of the first n 32-bit entries of a list or pool that starts on a
+// 16-byte boundary into another such range, rounded up to whole 16-byte
+// units (both ranges hold at least that many entries: capacities are powers
+// of two >= 4).
 __device__ __forceinline__ void warp_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n, int lane) {
-  for (uint32_t i = lane; i < n; i += 32) dst[i] = src[i];
+  warp_copy_v4(reinterpret_cast<uint4*>(dst), reinterpret_cast<const uint4*>(src), (n + 3) / 4, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -235,9 +253,8 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
 
   // --- relocations (old contents keep their order) ---
   if (P.new_ecap) {
-    EdgeRec* dst = S.edges + res[A_EDGE];
-    const EdgeRec* src = S.edges + M.eoff;
-    for (uint32_t i = lane; i < M.ecnt; i += 32) dst[i] = src[i];
+    warp_copy_v4(reinterpret_cast<uint4*>(S.edges + res[A_EDGE]), reinterpret_cast<const uint4*>(S.edges + M.eoff),
+                 M.ecnt, lane);
     M.eoff = res[A_EDGE];
     M.ecap = P.new_ecap;
   }
@@ -247,18 +264,22 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
     M.bpcap = P.new_bpcap;
   }
   {
-    uint32_t grow = __ballot_sync(kFull, P.gcap_lane != 0);
-    while (grow) {
-      const int k = __ffs(grow) - 1;
-      grow &= grow - 1;
-      const uint32_t ob = __shfl_sync(kFull, group_base(G), k), oc = __shfl_sync(kFull, G.cnt, k);
-      const unsigned long long nb = res[A_MEMBER] + __shfl_sync(kFull, P.gpre, k);  // entries
+    // Lists that move: the whole warp copies the members of each non-empty
+    // one in turn; every moving lane then takes its new base (a list that
+    // held no members needs no copy, the common case for a new group).
+    const uint32_t old_base = group_base(G);
+    uint32_t copy = __ballot_sync(kFull, P.gcap_lane != 0 && G.cnt != 0);
+    if (P.gcap_lane) {
+      G.base1 = (uint32_t)((res[A_MEMBER] + P.gpre) >> 2) + 1u;  // reserved offsets are 4-entry aligned
+      G.roomy = 0;
+    }
+    while (copy) {
+      const int k = __ffs(copy) - 1;
+      copy &= copy - 1;
+      const uint32_t ob = __shfl_sync(kFull, old_base, k), oc = __shfl_sync(kFull, G.cnt, k);
+      const size_t nb = (size_t)__shfl_sync(kFull, group_base(G), k) * 4;
       warp_copy_u32(S.gv + nb, S.gv + (size_t)ob * 4, oc, lane);
       warp_copy_u32(S.gs + nb, S.gs + (size_t)ob * 4, oc, lane);
-      if (lane == k) {
-        G.base1 = (uint32_t)(nb >> 2) + 1u;
-        G.roomy = 0;
-      }
     }
   }
   if (P.new_acap) {
