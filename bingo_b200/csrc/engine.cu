@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
   }
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
+__global__ void __launch_bounds__(kBlock, 3) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, const uint32_t* ctl) {
   __shared__ uint32_t stage[kBlock / 32][64];

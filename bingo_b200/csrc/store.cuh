@@ -398,6 +398,9 @@ __device__ __forceinline__ void plan_append(const StoreView& S, uint32_t u, cons
   need[A_HASH] = P.new_hcap;
 }
 
+// Removals of one group a lane resolves per round of loads (apply_delete).
+constexpr int kDeleteRound = 4;
+
 // ---------------------------------------------------------------------------
 // Delete a run of slots of one vertex in batch order. Each delete swap-removes
 // the slot from every group its weight has a bit in (lane k = group k) and
@@ -440,20 +443,62 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
       const int d = __ffs(r) - 1;
       if ((stage[d] >> lane) & 1u) mine |= 1u << d;
     }
+    // Up to kDeleteRound removals at a time: their members' positions, the
+    // list's last entries and those entries' edge records are loaded
+    // together (two rounds of loads), then the swap-removes run in
+    // registers, in batch order, and are stored. A removal whose member was
+    // moved by an earlier one, or a last entry that an earlier removal
+    // overwrote, is followed in registers (entries are told apart by their
+    // back-pointer index, which is unique per (slot, bit)).
+    uint32_t* const bpv = S.bp + M.bpoff;
     while (mine) {
-      const int d = __ffs(mine) - 1;
-      mine &= mine - 1;
-      const uint32_t w = stage[d], ebp = stage[32 + d];
-      const uint32_t pos = S.bp[M.bpoff + ebp + __popc(w & below)];
-      const uint32_t last = G.cnt - 1;
-      const uint32_t ms = S.gs[gb + last];
-      const uint32_t mv = S.gv[gb + last];
-      S.gv[gb + pos] = mv;
-      S.gs[gb + pos] = ms;
-      if (pos == 0) front_known = true, front = mv;
-      const EdgeRec em = S.edges[M.eoff + ms];
-      S.bp[M.bpoff + em.ebp + __popc(em.w & below)] = pos;
-      G.cnt = last;
+      uint32_t bpi[kDeleteRound], pos[kDeleteRound], ts[kDeleteRound], tv[kDeleteRound], tbi[kDeleteRound];
+      int r = 0;
+#pragma unroll
+      for (int q = 0; q < kDeleteRound; ++q) {
+        bpi[q] = 0;
+        if (mine) {
+          const int d = __ffs(mine) - 1;
+          mine &= mine - 1;
+          bpi[q] = stage[32 + d] + __popc(stage[d] & below);
+          r = q + 1;
+        }
+      }
+      const uint32_t c0 = G.cnt;  // >= r: every removal's member is in the list
+#pragma unroll
+      for (int q = 0; q < kDeleteRound; ++q) {
+        pos[q] = ts[q] = tv[q] = tbi[q] = 0;
+        if (q < r) {
+          pos[q] = bpv[bpi[q]];
+          ts[q] = S.gs[gb + c0 - 1 - q];
+          tv[q] = S.gv[gb + c0 - 1 - q];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kDeleteRound; ++q) {
+        if (q < r) {
+          const EdgeRec em = S.edges[M.eoff + ts[q]];
+          tbi[q] = em.ebp + __popc(em.w & below);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kDeleteRound; ++i) {
+        if (i < r) {
+          // Removal i: the entry at the current last position (c0 - 1 - i)
+          // moves into the removed member's position p.
+          const uint32_t p = pos[i], ms = ts[i], mv = tv[i], mbi = tbi[i];
+          S.gv[gb + p] = mv;
+          S.gs[gb + p] = ms;
+          bpv[mbi] = p;
+          if (p == 0) front_known = true, front = mv;
+#pragma unroll
+          for (int t = i + 1; t < kDeleteRound; ++t) {
+            if (t < r && p == c0 - 1 - t) ts[t] = ms, tv[t] = mv, tbi[t] = mbi;  // a later last entry
+            if (t < r && bpi[t] == mbi) pos[t] = p;                              // a later removal moved
+          }
+        }
+      }
+      G.cnt = c0 - r;
     }
     __syncwarp();
     if (valid) {
