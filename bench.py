@@ -10,6 +10,14 @@ device-timed step (updates included), inputs resident in HBM; `e2e` = the same
 metric through the C ABI with pinned host buffers (batches copied in, every
 walk row copied out, inside the timed region). With N > 1 (torchrun) every
 rank runs a full replica (weak scaling, no collective on the data path).
+
+At N = 1 the default run also measures, each in a child process with its own
+clock record, the node2vec workload (R-MAT 22), the batched form against the
+plain form (256 mixed jobs on R-MAT 22), the served form against the plain
+form (Poisson requests on R-MAT 24) and the reference's own CUDA build on the
+DeepWalk workload with weights below 2^16, and reports them under
+`other_workloads` (`--no-extras` skips them; they never run under a
+profiler).
 """
 from __future__ import annotations
 

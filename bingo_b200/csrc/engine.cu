@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
                                                          unsigned long long k, uint32_t ks, const uint32_t* ctl,
                                                          const ArenaNeed* scan,
                                                          const unsigned long long* base, uint32_t* out_slots) {
+  __shared__ AliasScratch asc[kBlock / 32];
   if (*ctl) return;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
   const uint32_t nS = *nseg;
@@ -186,13 +187,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
     unsigned long long res[kArenas];
 #pragma unroll
     for (int a = 0; a < kArenas; ++a) res[a] = base[a] + off.v[a];
-    apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res);
+    apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res, &asc[threadIdx.x / 32]);
   }
 }
 
 __global__ void __launch_bounds__(kBlock, 3) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, const uint32_t* ctl) {
+  __shared__ AliasScratch asc[kBlock / 32];
   __shared__ uint32_t stage[kBlock / 32][64];
   if (*ctl) return;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply_delete(StoreView S, const u
     seg_bounds(seg, nS, s, k, &b, &e);
     const uint32_t u = skey[b];
     if (u >= S.n) continue;
-    apply_delete(S, u, sslot + b, e - b, stage[threadIdx.x / 32]);
+    apply_delete(S, u, sslot + b, e - b, stage[threadIdx.x / 32], &asc[threadIdx.x / 32]);
   }
 }
 

@@ -17,9 +17,16 @@ namespace bingo {
 // include/Bingo.cuh:111-158.
 //
 // single: the member of this lane's group when cnt == 1 (the table names a
-// one-member group by its member, AliasRec).
+// one-member group by its member, AliasRec). sc: this warp's shared-memory
+// scratch for the pairing loop.
+struct AliasScratch {
+  unsigned long long s[kBits];    // scaled masses
+  unsigned long long thr[kBits];  // thresholds out
+  uint8_t al[kBits];              // alias groups out
+};
+
 __device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uint32_t base, uint32_t single,
-                                                     AliasRec* out) {
+                                                     AliasRec* out, AliasScratch* sc) {
   const unsigned long long mass = (unsigned long long)cnt << lane;
   const uint32_t nz = __ballot_sync(kFull, cnt != 0);
   const uint32_t m = __popc(nz);
@@ -28,24 +35,42 @@ __device__ __forceinline__ uint32_t warp_build_alias(int lane, uint32_t cnt, uin
   unsigned long long thr = T;
   int alias_lane = lane;
   if (T < (1ull << 58)) {
-    // Every scaled mass is below 32 * 2^58: the same pairing in 64 bits.
-    unsigned long long s = mass * m;
+    // Every scaled mass is below 32 * 2^58: the pairing in 64 bits, run by
+    // lane 0 over shared memory (about half the instructions of a
+    // shuffle-per-step loop). The lowest large group stays the partner until
+    // it turns small (larges are never added), so its residual lives in a
+    // register meanwhile.
+    const unsigned long long s = mass * m;
     uint32_t small = __ballot_sync(kFull, cnt != 0 && s < T);
     uint32_t large = nz & ~small;
-    while (small && large) {
-      const int a = __ffs(small) - 1, b = __ffs(large) - 1;
-      const unsigned long long sa = __shfl_sync(kFull, s, a);
-      if (lane == a) {
-        thr = sa;
-        alias_lane = b;
+    if (small && large) {
+      sc->s[lane] = s;
+      sc->thr[lane] = T;
+      sc->al[lane] = (uint8_t)lane;
+      __syncwarp();
+      if (lane == 0) {
+        int b = -1;
+        unsigned long long sb = 0;
+        while (small && large) {
+          const int a = __ffs(small) - 1;
+          if (b < 0) b = __ffs(large) - 1, sb = sc->s[b];
+          const unsigned long long sa = sc->s[a];
+          sc->thr[a] = sa;
+          sc->al[a] = (uint8_t)b;
+          sb -= T - sa;
+          small &= ~(1u << a);
+          if (sb < T) {
+            sc->s[b] = sb;
+            large &= ~(1u << b);
+            small |= 1u << b;
+            b = -1;
+          }
+        }
       }
-      if (lane == b) s -= T - sa;
-      small &= ~(1u << a);
-      const bool b_small = __shfl_sync(kFull, (int)(s < T), b);
-      if (b_small) {
-        large &= ~(1u << b);
-        small |= 1u << b;
-      }
+      __syncwarp();
+      thr = sc->thr[lane];
+      alias_lane = sc->al[lane];
+      __syncwarp();  // the scratch is reused by this warp's next vertex
     }
   } else {
     unsigned __int128 s = (unsigned __int128)mass * m;
@@ -237,7 +262,7 @@ __device__ __forceinline__ void warp_copy_u32(uint32_t* dst, const uint32_t* src
 // this segment (units of each arena).
 static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32_t* seg_v, const uint32_t* seg_w,
                              const uint32_t* seg_orig, uint32_t len, uint32_t* out_slots,
-                             const unsigned long long res[kArenas]) {
+                             const unsigned long long res[kArenas], AliasScratch* sc) {
   const int lane = threadIdx.x & 31;
   VertexMeta M = S.meta[u];
   GroupDesc G = S.gdesc[(size_t)u * kBits + lane];
@@ -372,7 +397,7 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
   __syncwarp();
 
   // --- alias table over the new counts ---
-  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff);
+  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff, sc);
   if (add_lane && !P.gcap_lane) G.roomy = group_roomy(G.cnt, cap0);
   if (add_lane || P.gcap_lane) S.gdesc[(size_t)u * kBits + lane] = G;  // only the descriptors that changed
   if (lane == 0) {
@@ -414,7 +439,7 @@ constexpr int kDeleteRound = 4;
 // (include/Bingo.cuh:199-218) and deleteKernel (include/operation.cuh:198-214).
 // stage: 64 words of shared memory owned by this warp.
 static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32_t* seg_slot, uint32_t len,
-                                    uint32_t* stage) {
+                                    uint32_t* stage, AliasScratch* sc) {
   const int lane = threadIdx.x & 31;
   const uint32_t below = lanemask_lt();
   VertexMeta M = S.meta[u];
@@ -514,7 +539,7 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
   }
   // A group left with one member is named by it in the alias table.
   const uint32_t single = G.cnt == 1 ? (front_known ? front : S.gv[gb]) : 0u;
-  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff);
+  R.m = warp_build_alias(lane, G.cnt, group_base(G), single, S.alias + R.aoff, sc);
   if (G.cnt != cnt0) {  // only the descriptors that changed
     G.roomy = group_roomy(G.cnt, cap0);
     S.gdesc[(size_t)u * kBits + lane] = G;
