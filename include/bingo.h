@@ -270,7 +270,12 @@ int bingo_serve_start(bingo_handle* h, const bingo_serve_config* cfg);
 int bingo_serve_submit_walk(bingo_handle* h, const bingo_walk_job* job, uint64_t* ticket);
 /* kind: BINGO_OP_INSERT (a = src, b = dst, c = weights, out_slots optional),
  * BINGO_OP_DELETE (a = vertex, b = slot) or BINGO_OP_DELETE_PAIRS (a = u,
- * b = v, as bingo_delete_pairs). */
+ * b = v, as bingo_delete_pairs). The batch is copied at submission. It
+ * applies after every walk submitted before it has finished on the device
+ * and before any walk submitted after it starts; its ticket is done once the
+ * batch has applied, with the batch's own status (a delete batch with absent
+ * or repeated slots applies the rest and reports BINGO_ERR_INVALID_SLOT).
+ * out_slots (host memory) holds the slot ids once the ticket is done. */
 int bingo_serve_submit_update(bingo_handle* h, int32_t kind, const uint32_t* a, const uint32_t* b,
                               const uint32_t* c, uint64_t k, uint32_t* out_slots, uint64_t* ticket);
 int bingo_serve_poll(bingo_handle* h, uint64_t ticket, bingo_serve_status* out);

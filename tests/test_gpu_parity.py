@@ -273,3 +273,55 @@ def test_cuda_state_matches_reference_binary(path):
             g.delete_batch(z[f"op{i}_a"], z[f"op{i}_b"])
         ref = {k: z[f"dump{i}_{k}"] for k in names}
         compare_exact_vs_ref(g.dump(), ref, n, check_alias_tol=5e-3)
+
+
+def test_group_lists_shrink_and_regrow(tmp_path):
+    """Group capacity is derived from the count plus a hysteresis bit: a list
+    whose count dips below a power of two and climbs back keeps its storage
+    (no move per cycle), a deep dip followed by regrowth moves it, and the
+    state stays equal to the oracle's throughout."""
+    from tests.test_gpu_check import Snap
+    n = 64
+    src = np.zeros(20, np.uint32)
+    dst = np.arange(1, 21, dtype=np.uint32)
+    w = np.ones(20, np.uint32)  # every edge in group 0 only: its count is vertex 0's degree
+    src = np.concatenate([src, np.arange(1, 40, dtype=np.uint32)])
+    dst = np.concatenate([dst, np.arange(2, 41, dtype=np.uint32)])
+    w = np.concatenate([w, gen.weights(39, gen.W_UNIFORM, 1, 1000, seed=7)])
+    g, ex = Graph(node2vec=True), po.ExactGraph(n)
+    g.load_edges(src, dst, w, n)
+    ex.load(src, dst, w)
+    live = list(range(20))  # live slots of vertex 0
+
+    def group0():
+        p = tmp_path / "s.snap"
+        g.save(p)
+        return Snap(p.read_bytes()).group(0, 0)
+
+    def cycle(k, seed):
+        rng = np.random.default_rng(seed)
+        pick = sorted(rng.choice(len(live), size=k, replace=False).tolist(), reverse=True)
+        slots = np.array([live.pop(i) for i in pick], np.uint32)
+        u = np.zeros(k, np.uint32)
+        g.delete_batch(u, slots)
+        assert ex.delete(u, slots) == 0
+        assert_exact_equal(g.dump(), ex.dump(), f"after deleting {k}: ")
+        v = rng.integers(1, n, size=k).astype(np.uint32)
+        ins = (u, v, np.ones(k, np.uint32))
+        got = g.insert_batch(*ins)
+        assert np.array_equal(got, ex.insert(*ins))
+        live.extend(got.tolist())
+        assert_exact_equal(g.dump(), ex.dump(), f"after reinserting {k}: ")
+
+    base0, cnt0, cap0 = group0()
+    assert cnt0 == 20 and cap0 == 32
+    for c in range(6):  # 20 -> 15 -> 20: below 16 and back, within the list's 32 entries
+        cycle(5, 100 + c)
+        base, cnt, cap = group0()
+        assert (base, cnt) == (base0, 20), f"cycle {c}: the list moved ({base0} -> {base})"
+    for c in range(3):  # 20 -> 3 -> 20: the deep dip forgets the spare room, regrowth moves the list
+        cycle(17, 200 + c)
+        assert group0()[1] == 20
+    assert g.check()["bad_vertices"] == 0
+    walks = g.walk(app=DEEPWALK, length=30, starts=np.arange(n, dtype=np.uint32), seed=3)
+    assert np.array_equal(walks, ex.walk(DEEPWALK, 30, np.arange(n, dtype=np.uint32), seed=3))

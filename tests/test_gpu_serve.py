@@ -143,3 +143,41 @@ def test_stalled_producer_and_bad_update():
     assert np.array_equal(out1, ref.walk(app=DEEPWALK, length=30, starts=st1, seed=1, job_id=1))
     assert np.array_equal(out2, ref.walk(app=DEEPWALK, length=30, starts=st2, seed=2, job_id=2))
     assert g.stats()["live_edges"] == len(src)
+
+
+def test_update_status_and_back_to_back_updates():
+    """Updates commit without a host wait: a delete batch holding an absent
+    slot (a repeated delete) reports BINGO_ERR_INVALID_SLOT on its own ticket
+    once its valid deletes have applied; two updates submitted back to back
+    apply in order; a query submitted right after them sees both, and the
+    store ends equal to the oracle's."""
+    n, src, dst, w = _graph(scale=11, seed=99)
+    g = Graph()
+    g.load_edges(src, dst, w, n)
+    ex = po.ExactGraph(n)
+    ex.load(src, dst, w)
+    ug = gen.UpdateGen(n, src, dst, seed=100)
+    rng = np.random.default_rng(101)
+    g.serve_start(idle_timeout_us=2000)
+    warm = rng.integers(0, n, size=200).astype(np.uint32)
+    t0, out0 = g.submit_walk(app=DEEPWALK, length=20, starts=warm, seed=5, job_id=5)
+    ins = ug.inserts(500, gen.W_UNIFORM, 1, 65535)
+    t1, slots = g.submit_update("insert", *ins)
+    du, ds = ug.deletes(300)
+    du = np.concatenate([du, du[:1]]).astype(np.uint32)  # the repeat is an absent slot: skipped, reported
+    ds = np.concatenate([ds, ds[:1]]).astype(np.uint32)
+    t2, _ = g.submit_update("delete", du, ds)
+    starts = rng.integers(0, n, size=1500).astype(np.uint32)
+    t3, out3 = g.submit_walk(app=PPR, length=40, starts=starts, seed=6, job_id=6, stop_prob=0.15)
+    s0, s1, s2, s3 = (g.serve_wait(t) for t in (t0, t1, t2, t3))
+    g.serve_stop()
+    assert s0["status"] == 0 and s0["version"] == 0
+    assert s1["status"] == 0 and s1["version"] == 1
+    assert s2["status"] == 4 and s2["version"] == 2  # BINGO_ERR_INVALID_SLOT
+    assert s3["status"] == 0 and s3["version"] == 2
+    assert np.array_equal(out0, ex.walk(DEEPWALK, 20, warm, seed=5, job_id=5))
+    assert np.array_equal(slots, ex.insert(*ins))
+    assert ex.delete(du, ds) == 1
+    assert np.array_equal(out3, ex.walk(PPR, 40, starts, seed=6, job_id=6, stop=0.15))
+    from tests.helpers import assert_exact_equal
+    assert_exact_equal(g.dump(), ex.dump())
