@@ -293,7 +293,7 @@ static_assert(kBlock % 32 == 0, "whole warps");
 constexpr int walk_min_blocks(int app, bool multi) {
   return app == APP_DEEPWALK || app == APP_SAMPLING ? 8
          : app == APP_PPR                           ? (multi ? 5 : 6)
-         : app == APP_NODE2VEC                      ? (multi ? 4 : 6)
+         : app == APP_NODE2VEC                      ? (multi ? 4 : 5)
                                                     : 4;
 }
 
