@@ -1,5 +1,5 @@
-"""Bit-exact parity at the full size of the two plain-form workloads, against
-the CPU oracle (ExactGraph) fed the same inputs.
+"""Bit-exact parity at the full size of the DeepWalk, node2vec and batched
+workloads, against the CPU oracle (ExactGraph) fed the same inputs.
 
 DeepWalk workload: R-MAT scale 20 (16.1 M edges), log-uniform weights in
 [1, 2^20), the bench's own generator and batches. After the load and after
@@ -87,4 +87,50 @@ def test_node2vec_rmat22_state_after_batch_and_walk_sample():
     ref = ex.walk(NODE2VEC, L, starts, seed=seed, job_id=job, p=0.5, q=2.0)
     bad = np.nonzero((rows != ref).any(axis=1))[0]
     assert len(bad) == 0, f"{len(bad)} of {len(starts)} walks differ, first {bad[:5]}"
+    g.close()
+
+
+def test_batched_program_rmat22_phase():
+    """Batched workload at full size: R-MAT scale 22 (65 M edges), uniform
+    [1, 65535] weights, the first phase's 16 mixed jobs (DeepWalk, node2vec
+    with p, q in {0.25, 1, 4}, PPR stop 0.15; start sets of 1K-1M, lengths
+    5-200) and its update chunk, run as one captured program (walks, insert,
+    delete). The first 4,096 rows of every job equal the oracle's on the
+    graph before the chunk, the chunk's slot ids equal the oracle's, and the
+    whole store after it equals the oracle's."""
+    import torch
+
+    import bench
+    from bingo_b200 import WalkJob as WJ
+    n, src, dst, w, jobs, chunk, steps = bench.make_batched_workload(1)
+    g = Graph(node2vec=True)
+    ex = po.ExactGraph(n)
+    g.load_edges(src, dst, w, n)
+    ex.load(src, dst, w)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+    phase = jobs[:bench.B_JOBS_PER_PHASE]
+    ins, dels = steps[0][0]
+    starts = [dev(J["starts"]) for J in phase]
+    outs = [torch.empty((len(J["starts"]), J["length"]), dtype=torch.int32, device="cuda") for J in phase]
+    slots = torch.empty(len(ins[0]), dtype=torch.int32, device="cuda")
+    seed = 77
+    walk_jobs = [WJ(app=J["app"], length=J["length"], starts=starts[k], n_starts=len(J["starts"]), job_id=J["job_id"],
+                    seed=seed, p=J["p"], q=J["q"], stop_prob=J["stop_prob"], out=outs[k]) for k, J in enumerate(phase)]
+    g.run([("walk", walk_jobs), ("insert", dev(ins[0]), dev(ins[1]), dev(ins[2]), slots),
+           ("delete", dev(dels[0]), dev(dels[1]))], graph=True)
+    g.sync()
+    K = 4096
+    for k, J in enumerate(phase):
+        st = np.ascontiguousarray(J["starts"][:K], dtype=np.uint32)
+        ref = ex.walk(J["app"], J["length"], st, seed=seed, job_id=J["job_id"], p=J["p"], q=J["q"],
+                      stop=J["stop_prob"])
+        got = outs[k][:len(st)].cpu().numpy()
+        bad = np.nonzero((got != ref).any(axis=1))[0]
+        assert len(bad) == 0, f"job {J['job_id']} (app {J['app']}, p {J['p']}, q {J['q']}): rows {bad[:5]} differ"
+    assert np.array_equal(slots.cpu().numpy().view(np.uint32), ex.insert(*ins)), "chunk slot ids"
+    assert ex.delete(*dels) == 0
+    _compare_state(g, ex, "after the chunk: ")
     g.close()
