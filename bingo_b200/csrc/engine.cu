@@ -387,39 +387,54 @@ unsigned walk_blocks_per_sm() {
   return (unsigned)b;
 }
 
-// Blocks per SM for a walk launch: the tuned figure capped by occupancy
-// (0 = occupancy).
-unsigned walk_bps(unsigned occ, const Tuning& t) {
-  return t.walk_blocks_per_sm ? std::max(1u, std::min(occ, t.walk_blocks_per_sm)) : occ;
+// Default launch shape of each walk kernel (the knobs' value 0), measured on
+// B200 with fixed graphs, launches interleaved: resident 256-thread blocks
+// per SM (0 = the occupancy limit) and walks a warp claims per refill.
+// DeepWalk (config 2's graph): 26.3 G steps/s at 4 blocks and 8 walks
+// against 21.7 G at its 8-block occupancy limit and 32 (more resident warps
+// issue more concurrent random reads than DRAM turns into throughput; 2
+// blocks: 23.0 G). PPR: 11.3 G at 4 blocks and 32 against 11.0 G at 6.
+// node2vec (config 3's graph) and the mixed-app table (config 4's jobs) run
+// best at their occupancy limits (5 and 4 blocks) with 32. One-hop sampling
+// (one step per item) keeps the occupancy limit and 32.
+constexpr unsigned walk_default_bps(int app) { return app == APP_DEEPWALK || app == APP_PPR ? 4 : 0; }
+constexpr uint32_t walk_default_chunk(int app) { return app == APP_DEEPWALK ? 8 : 32; }
+
+// Blocks per SM for a walk launch of `app` (-1: mixed table): the tuned or
+// default figure, capped by occupancy.
+unsigned walk_bps(unsigned occ, const Tuning& t, int app) {
+  const unsigned want = t.walk_blocks_per_sm ? t.walk_blocks_per_sm : walk_default_bps(app);
+  return want ? std::max(1u, std::min(occ, want)) : occ;
 }
+uint32_t walk_chunk_of(const Tuning& t, int app) { return t.walk_chunk ? t.walk_chunk : walk_default_chunk(app); }
 
 // Launches the persistent walk kernel for a device job table whose jobs all
 // have app `app` (or any app when app < 0).
 void launch_walk_table(cudaStream_t st, int app, const WalkView& W, const WalkJobDev& J0, const WalkJobDev* jobs,
                        const uint32_t* prefix, uint32_t n_jobs, uint32_t total, uint32_t* queue, const Tuning& t) {
-  const uint32_t c = t.walk_chunk;
+  const uint32_t c = walk_chunk_of(t, app);
   switch (app) {
     case APP_DEEPWALK:
       k_walk<APP_DEEPWALK, true>
-          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_DEEPWALK, true>(), t)), kBlock, 0, st>>>(
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_DEEPWALK, true>(), t, APP_DEEPWALK)), kBlock, 0, st>>>(
               W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_NODE2VEC:
       k_walk<APP_NODE2VEC, true>
-          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_NODE2VEC, true>(), t)), kBlock, 0, st>>>(
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_NODE2VEC, true>(), t, APP_NODE2VEC)), kBlock, 0, st>>>(
               W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_PPR:
-      k_walk<APP_PPR, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_PPR, true>(), t)), kBlock, 0, st>>>(
+      k_walk<APP_PPR, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_PPR, true>(), t, APP_PPR)), kBlock, 0, st>>>(
           W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     case APP_SAMPLING:
       k_walk<APP_SAMPLING, true>
-          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_SAMPLING, true>(), t)), kBlock, 0, st>>>(
+          <<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<APP_SAMPLING, true>(), t, APP_SAMPLING)), kBlock, 0, st>>>(
               W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
     default:
-      k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), t)), kBlock, 0, st>>>(
+      k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), t, -1)), kBlock, 0, st>>>(
           W, J0, jobs, prefix, n_jobs, total, queue, c);
       break;
   }
@@ -1220,10 +1235,11 @@ void Engine::walk(const bingo_walk_job* jobs, uint32_t n_jobs, uint32_t mode) {
   auto launch = [&](auto kern, unsigned occ, const WalkJobDev& J0, const WalkJobDev* jb, const uint32_t* pf,
                     uint32_t nj, uint32_t tot, uint32_t* qq) {
     cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(grid_for(tot, kBlock, walk_bps(occ, tuning_)));
+    lc.gridDim = dim3(grid_for(tot, kBlock, walk_bps(occ, tuning_, J0.app)));
     lc.blockDim = dim3(kBlock);
     lc.stream = stream_;
-    cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq, tuning_.walk_chunk), "walk launch");
+    cuda_check(cudaLaunchKernelEx(&lc, kern, W, J0, jb, pf, nj, tot, qq, walk_chunk_of(tuning_, J0.app)),
+               "walk launch");
     ++launches_;
   };
   queue_.ensure(4 * std::max<uint32_t>(n_jobs, 4), "walk queue");
@@ -1679,8 +1695,8 @@ void Engine::walk_noalloc(const bingo_walk_job* jobs, uint32_t n_jobs) {
   cuda_check(cudaGetLastError(), "no-alloc job staging");
   ++launches_;
   const WalkView W = wview();
-  k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), tuning_)), kBlock, 0, stream_>>>(
-      W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue, tuning_.walk_chunk);
+  k_walk<-1, true><<<grid_for(total, kBlock, walk_bps(walk_blocks_per_sm<-1, true>(), tuning_, -1)), kBlock, 0, stream_>>>(
+      W, dj[0], scratch->jobs, scratch->prefix, n_jobs, (uint32_t)total, &scratch->queue, walk_chunk_of(tuning_, -1));
   cuda_check(cudaGetLastError(), "no-alloc walk launch");
   ++launches_;
   finish_call();
@@ -1854,7 +1870,7 @@ void StateCopy::release() {
 }
 
 void Engine::set_tuning(const Tuning& t) {
-  if (t.walk_chunk < 1 || t.walk_chunk > 1024) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_chunk must be in [1, 1024]");
+  if (t.walk_chunk > 1024) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_chunk must be in [0, 1024] (0: the kernel's default)");
   if (t.walk_blocks_per_sm > 32) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_blocks_per_sm must be <= 32");
   if (t.walk_split > 1 || t.walk_order > 1) throw Error(BINGO_ERR_INVALID_ARGUMENT, "walk_split / walk_order are 0 or 1");
   if (t.apply_blocks_per_sm < 1 || t.apply_blocks_per_sm > 32)

@@ -50,8 +50,8 @@ class Server;
 
 // Launch and batching knobs (bingo_tuning); none changes any result.
 struct Tuning {
-  uint32_t walk_chunk = 32;
-  uint32_t walk_blocks_per_sm = 0;  // 0 = occupancy limit
+  uint32_t walk_chunk = 0;          // 0 = each walk kernel's default (walk_default_chunk)
+  uint32_t walk_blocks_per_sm = 0;  // 0 = each walk kernel's default (walk_default_bps)
   uint32_t walk_split = 0;
   uint32_t walk_order = 1;
   uint32_t update_chunk = 0;  // 0 = whole batch

@@ -78,10 +78,10 @@ void Engine::autotune(const bingo_tune_request& R, bingo_tune_report* out) {
       for (uint32_t j = 1; j < R.n_jobs; ++j) mixed |= R.jobs[j].app != R.jobs[0].app;
       if (mixed) try_knob(&Tuning::walk_split, {0, 1});
       if (R.n_jobs > 1) try_knob(&Tuning::walk_order, {1, 0});
-      try_knob(&Tuning::walk_blocks_per_sm, {0, 6, 4, 2});
-      std::vector<uint32_t> around;
+      try_knob(&Tuning::walk_blocks_per_sm, {0, 6, 4, 3, 2});
+      std::vector<uint32_t> around;  // 0 (each kernel's default) has no neighbours
       if (best.walk_chunk > 1) around.push_back(best.walk_chunk / 2);
-      if (best.walk_chunk < 1024) around.push_back(best.walk_chunk * 2);
+      if (best.walk_chunk && best.walk_chunk < 1024) around.push_back(best.walk_chunk * 2);
       try_knob(&Tuning::walk_chunk, around);
     } catch (...) {
       tuning_ = start;

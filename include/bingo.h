@@ -340,8 +340,11 @@ int bingo_check(bingo_handle* h, bingo_check_report* out);
  * Launch and batching parameters. None of them changes any result (walks,
  * slot ids, graph state); bingo_autotune picks them by measurement. */
 typedef struct bingo_tuning {
-  uint32_t walk_chunk;          /* walks a warp claims per refill, 1..1024 (default 32) */
-  uint32_t walk_blocks_per_sm;  /* resident walk blocks per SM, 0 = the occupancy limit (default) */
+  uint32_t walk_chunk;          /* walks a warp claims per refill, 1..1024; 0 (default) = each walk
+                                   kernel's measured default: 8 for DeepWalk, 32 otherwise */
+  uint32_t walk_blocks_per_sm;  /* resident walk blocks per SM, capped by occupancy; 0 (default) =
+                                   each walk kernel's measured default: 4 for DeepWalk and PPR, the
+                                   occupancy limit otherwise */
   uint32_t walk_split;          /* 1: one persistent launch per app; 0: one mixed launch (default) */
   uint32_t walk_order;          /* 1: jobs with the longest expected walks first (default); 0: job order */
   uint32_t update_chunk;        /* edges per update sub-batch of bingo_insert_batch / bingo_delete_batch,

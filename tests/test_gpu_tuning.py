@@ -110,7 +110,7 @@ def test_invalid_tuning_rejected():
     n, src, dst, w, _ = workload(scale=8, ef=4, seed=2, rounds=0)
     g = Graph()
     g.load_edges(src, dst, w, n)
-    for bad in (dict(walk_chunk=0), dict(walk_chunk=2048), dict(apply_blocks_per_sm=0), dict(walk_split=2)):
+    for bad in (dict(walk_chunk=1025), dict(walk_chunk=2048), dict(apply_blocks_per_sm=0), dict(walk_split=2)):
         with pytest.raises(BingoError):
             g.set_tuning(**bad)
     with pytest.raises(ValueError):
