@@ -714,7 +714,7 @@ def run_node2vec(args):
 EXTRA_RUNS = {
     "node2vec_cfg3": ["bench.py", "--workload", "node2vec", "--steps", "3", "--warmup", "3", "--no-cpu"],
     "batched_cfg4": ["bench.py", "--workload", "batched", "--steps", "3", "--warmup", "3"],
-    "served_cfg5": ["bench.py", "--workload", "served", "--rates", "4000,16000", "--requests", "1200"],
+    "served_cfg5": ["bench.py", "--workload", "served", "--rates", "4000,8000,16000", "--requests", "1200"],
     "reference_cuda_cfg2": ["oracle/compare_reference_cuda.py", "--workload", "plain", "--steps", "3",
                             "--warmup", "3"],
 }
