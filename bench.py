@@ -80,9 +80,9 @@ def peak_hbm():
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per produced step
 # of k_walk<DEEPWALK> on this workload, from one ncu capture of one launch:
 # the 4th walk launch of `bench.py --steps 3 --warmup 3` (the first timed
-# step, 31,776,603 produced steps; 2.800 GB read + 0.334 GB written).
+# step, 31,776,603 produced steps; 2.796 GB read + 0.334 GB written).
 # roofline.traffic scales it to the live run's steps per launch.
-WALK_DRAM_BYTES_PER_STEP = 98.6
+WALK_DRAM_BYTES_PER_STEP = 98.5
 WALK_DRAM_SOURCE = ("ncu capture of one k_walk<DEEPWALK> launch (4th launch, 31,776,603 steps) of "
                     "bench.py --steps 3 --warmup 3, scaled to this run's steps per launch")
 
