@@ -1,11 +1,13 @@
 // Engine: kernels and host orchestration for load / insert / delete / walk.
 //
-// Update batches run as: validate -> stable radix sort by vertex (CUB) ->
-// gather + segment heads -> segment list -> plan (per-vertex growth sizes) ->
-// exclusive scans per arena -> reserve -> apply (warp per vertex). Arena
-// offsets come from scans, so the layout is a deterministic function of the
-// inputs; arenas are index-addressed and grow by reallocation on the host
-// before a batch that would not fit.
+// Update batches run as: group by vertex (batches up to kGroupMax edges: one
+// cluster kernel that validates, sorts stably and lists the segments; larger
+// ones: validate -> CUB radix sort -> gather + segment heads -> segment
+// select) -> plan (per-vertex growth sizes) -> exclusive scans per arena ->
+// reserve -> apply (warp per vertex). Arena offsets come from scans, so the
+// layout is a deterministic function of the inputs; arenas are
+// index-addressed and grow by reallocation on the host before a batch that
+// would not fit.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -16,6 +18,7 @@
 #include <mutex>
 
 #include "engine.cuh"
+#include "group.cuh"
 #include "serve.cuh"
 #include "store.cuh"
 #include "walk.cuh"
@@ -718,6 +721,7 @@ void Engine::ensure_batch_scratch(uint64_t k) {
   cub::DeviceScan::ExclusiveScan(nullptr, t_scan, (const ArenaNeed*)nullptr, (ArenaNeed*)nullptr, AddNeed(),
                                  ArenaNeed{}, (int)ks, stream_);
   cub_tmp_.ensure(std::max(t_sort, std::max(t_sel, t_scan)), "scratch");
+  group_cluster_ok();  // probed here, outside any stream capture
 }
 
 const uint32_t* Engine::stage(const uint32_t* p, uint64_t k, DevBuf& buf, const char* what) {
@@ -730,9 +734,42 @@ const uint32_t* Engine::stage(const uint32_t* p, uint64_t k, DevBuf& buf, const 
 // Stable sort of the batch by vertex; leaves sorted keys in key_s_, the
 // original index in perm_, payloads a/b in sorted order in sa_/sb_, and the
 // segment start list in seg_ with its count in nseg_.
-void Engine::group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k) {
+bool Engine::group_cluster_ok() {
+  if (group_cluster_ < 0) {
+    group_cluster_ = 0;
+    if (cudaFuncSetAttribute(k_group_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)group_smem_bytes(kGroupIpt)) == cudaSuccess) {
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3(kGroupCtas);
+      lc.blockDim = dim3(kGroupThreads);
+      lc.dynamicSmemBytes = group_smem_bytes(kGroupIpt);
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, k_group_small, &lc) == cudaSuccess && clusters > 0)
+        group_cluster_ = 1;
+    }
+    cudaGetLastError();  // a refused query leaves the CUB path in place, not a sticky error
+  }
+  return group_cluster_ == 1;
+}
+
+void Engine::group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k, bool insert) {
   int end_bit = 1;
   while (end_bit < 32 && (1ull << end_bit) < n_) ++end_bit;
+  if (k >= 1 && k <= kGroupMax && group_cluster_ok()) {
+    const uint32_t ipt = group_ipt(k);
+    k_group_small<<<kGroupCtas, kGroupThreads, group_smem_bytes(ipt), stream_>>>(
+        key, a, b, (uint32_t)k, n_, end_bit, ipt, insert ? 1 : 0, key_s_.as<uint32_t>(), perm_.as<uint32_t>(),
+        sa_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), ctl_.as<uint32_t>(),
+        d_err_);
+    cuda_check(cudaGetLastError(), "group batch");
+    ++launches_;
+    return;
+  }
+  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
+  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(key, insert ? a : nullptr, insert ? b : nullptr, k, n_,
+                                                              ctl_.as<uint32_t>(), d_err_);
+  cuda_check(cudaGetLastError(), "validate");
+  ++launches_;
   size_t tb = cub_tmp_.bytes;
   cuda_check(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tb, key, key_s_.as<uint32_t>(), iota_.as<uint32_t>(),
                                              perm_.as<uint32_t>(), (int)k, 0, end_bit, stream_),
@@ -919,11 +956,7 @@ void Engine::load(const uint32_t* src, const uint32_t* dst, const uint32_t* w, u
   const uint32_t* ds = stage(src, m, in_a_, "stage src");
   const uint32_t* dd = stage(dst, m, in_b_, "stage dst");
   const uint32_t* dw = stage(w, m, in_c_, "stage w");
-  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
-  k_validate<<<grid_for(m, kBlock, 16), kBlock, 0, stream_>>>(ds, dd, dw, m, n, ctl_.as<uint32_t>(), d_err_);
-  cuda_check(cudaGetLastError(), "validate");
-  ++launches_;
-  group_by_vertex(ds, dd, dw, m);
+  group_by_vertex(ds, dd, dw, m, true);
   run_insert(m, nullptr, true, m);
   loaded_ = true;
   // Release load-sized scratch; update batches re-grow what they need.
@@ -1031,11 +1064,7 @@ void Engine::insert_one(const uint32_t* src, const uint32_t* dst, const uint32_t
   const uint32_t* ds = stage(src, k, in_a_, "stage src");
   const uint32_t* dd = stage(dst, k, in_b_, "stage dst");
   const uint32_t* dw = stage(w, k, in_c_, "stage w");
-  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
-  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(ds, dd, dw, k, n_, ctl_.as<uint32_t>(), d_err_);
-  cuda_check(cudaGetLastError(), "validate");
-  ++launches_;
-  group_by_vertex(ds, dd, dw, k);
+  group_by_vertex(ds, dd, dw, k, true);
   const bool dev_out = out_slots && is_device_ptr(out_slots);
   uint32_t* dslots = out_slots ? (dev_out ? out_slots : slots_.as<uint32_t>()) : nullptr;
   run_insert(k, dslots, false, k);
@@ -1076,12 +1105,7 @@ void Engine::erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   ensure_batch_scratch(k);
   const uint32_t* du = stage(u, k, in_a_, "stage u");
   const uint32_t* dsl = stage(slot, k, in_b_, "stage slot");
-  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
-  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(du, nullptr, nullptr, k, n_, ctl_.as<uint32_t>(),
-                                                              d_err_);
-  cuda_check(cudaGetLastError(), "validate");
-  ++launches_;
-  group_by_vertex(du, dsl, nullptr, k);
+  group_by_vertex(du, dsl, nullptr, k, false);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
@@ -1372,11 +1396,7 @@ void Engine::drop_graph() {
 void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k,
                             uint32_t* out_slots) {
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
-  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
-  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(a, b, c, k, n_, ctl_.as<uint32_t>(), d_err_);
-  cuda_check(cudaGetLastError(), "validate");
-  ++launches_;
-  group_by_vertex(a, b, c, k);
+  group_by_vertex(a, b, c, k, true);
   const StoreView S = view();
   unsigned long long* d_tot = plan_needs(S, k, ks, nullptr);
   k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
@@ -1391,12 +1411,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
 }
 
 void Engine::enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k) {
-  cuda_check(cudaMemsetAsync(ctl_.p, 0, 16, stream_), "ctl");
-  k_validate<<<grid_for(k, kBlock, 16), kBlock, 0, stream_>>>(u, nullptr, nullptr, k, n_, ctl_.as<uint32_t>(),
-                                                              d_err_);
-  cuda_check(cudaGetLastError(), "validate");
-  ++launches_;
-  group_by_vertex(u, slot, nullptr, k);
+  group_by_vertex(u, slot, nullptr, k, false);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
