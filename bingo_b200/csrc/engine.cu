@@ -3,8 +3,9 @@
 // Update batches run as: group by vertex (batches up to kGroupMax edges: one
 // cluster kernel that validates, sorts stably and lists the segments; larger
 // ones: validate -> CUB radix sort -> gather + segment heads -> segment
-// select) -> plan (per-vertex growth sizes) -> exclusive scans per arena ->
-// reserve -> apply (warp per vertex). Arena offsets come from scans, so the
+// select) -> plan (per-vertex growth sizes, prefix inside each plan block) ->
+// prefix of the plan-block sums -> reserve -> apply (warp per vertex). Arena
+// offsets come from these prefix sums in segment order, so the
 // layout is a deterministic function of the inputs; arenas are
 // index-addressed and grow by reallocation on the host before a batch that
 // would not fit.
@@ -99,58 +100,124 @@ __device__ __forceinline__ void seg_bounds(const uint32_t* seg, uint32_t S, uint
   *e = s + 1 < S ? seg[s + 1] : (uint32_t)k;
 }
 
-// Arena sizes one segment needs (units of each arena); one exclusive scan
-// over these rows gives every segment its offsets in all arenas at once.
+// Arena sizes one segment needs (units of each arena).
 struct ArenaNeed {
   unsigned long long v[kArenas];
 };
-struct AddNeed {
-  __host__ __device__ ArenaNeed operator()(const ArenaNeed& a, const ArenaNeed& b) const {
-    ArenaNeed r;
-#pragma unroll
-    for (int i = 0; i < kArenas; ++i) r.v[i] = a.v[i] + b.v[i];
-    return r;
-  }
-};
 
-// Per-segment arena sizes (need[ks], zero past the last segment).
-__global__ void k_plan(StoreView S, const uint32_t* skey, const uint32_t* sw, const uint32_t* seg,
-                       const uint32_t* nseg, unsigned long long k, uint32_t ks, const uint32_t* ctl,
-                       ArenaNeed* need) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * blockDim.x / 32;
+// Plan blocks: one segment per warp, kPlanSegs consecutive segments per block.
+constexpr int kPlanThreads = 1024;
+constexpr int kPlanSegs = kPlanThreads / 32;
+constexpr int kTotalsThreads = 1024;
+
+// Plan blocks of a batch with ks segment slots.
+__host__ __device__ inline uint32_t plan_blocks(uint32_t ks) { return (ks + kPlanSegs - 1) / kPlanSegs; }
+
+// Per-segment arena sizes as an exclusive prefix inside the segment's plan
+// block (excl[s], s < ks) and each block's sums, column-major per arena
+// (bsum[a * nb + block]); segments past the last one need nothing. A
+// segment's offset in arena a is then the prefix of bsum over blocks (which
+// k_totals writes in place) plus excl[s].
+__global__ void __launch_bounds__(kPlanThreads) k_plan(StoreView S, const uint32_t* skey, const uint32_t* sw,
+                                                       const uint32_t* seg, const uint32_t* nseg,
+                                                       unsigned long long k, uint32_t ks, const uint32_t* ctl,
+                                                       ArenaNeed* excl, unsigned long long* bsum) {
+  __shared__ unsigned long long nd_s[kPlanSegs][kArenas];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t s = blockIdx.x * kPlanSegs + w;
   const uint32_t nS = *nseg;
-  const bool abort = *ctl != 0;
-  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < ks; s += warps) {
-    unsigned long long nd[kArenas] = {0, 0, 0, 0, 0};
-    if (!abort && s < nS) {
-      uint32_t b, e;
-      seg_bounds(seg, nS, s, k, &b, &e);
-      const uint32_t u = skey[b];
-      if (u < S.n) plan_append(S, u, sw + b, e - b, nd);
-    }
-    if (lane == 0) {
-      ArenaNeed r;
+  unsigned long long nd[kArenas] = {0, 0, 0, 0, 0};
+  if (*ctl == 0 && s < nS) {
+    uint32_t b, e;
+    seg_bounds(seg, nS, s, k, &b, &e);
+    const uint32_t u = skey[b];
+    if (u < S.n) plan_append(S, u, sw + b, e - b, nd);
+  }
+  if (lane == 0) {
 #pragma unroll
-      for (int a = 0; a < kArenas; ++a) r.v[a] = nd[a];
-      need[s] = r;
+    for (int a = 0; a < kArenas; ++a) nd_s[w][a] = nd[a];
+  }
+  __syncthreads();
+  if (w == 0) {  // lane v: the block's segment v
+    const uint32_t nb = plan_blocks(ks), sv = blockIdx.x * kPlanSegs + lane;
+#pragma unroll
+    for (int a = 0; a < kArenas; ++a) {
+      const unsigned long long y = nd_s[lane][a];
+      unsigned long long yi = y;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long z = __shfl_up_sync(kFull, yi, o);
+        if (lane >= o) yi += z;
+      }
+      if (sv < ks) excl[sv].v[a] = yi - y;
+      if (lane == 31) bsum[(size_t)a * nb + blockIdx.x] = yi;
     }
   }
 }
 
-// Batch totals per arena from the scanned needs. With `out` (mapped host
-// memory) it also publishes the insert plan: out[0..5) totals, out[5] the
-// batch status word, out[6..11) the arena tops.
-__global__ void k_totals(const ArenaNeed* need, const ArenaNeed* scan, uint32_t ks, unsigned long long* tot,
-                         const uint32_t* ctl, const unsigned long long* top, volatile unsigned long long* out) {
-  const int t = threadIdx.x;
-  const unsigned long long x = t < kArenas && ks ? scan[ks - 1].v[t] + need[ks - 1].v[t] : 0ull;
-  if (t < kArenas) tot[t] = x;
-  if (!out) return;
-  if (t < kArenas) out[t] = x;
-  if (t == kArenas) out[kArenas] = *ctl;
-  if (t < kArenas) out[kArenas + 1 + t] = top[t];
-  __threadfence_system();
+// Exclusive prefix of the nb plan-block sums (column-major per arena), in
+// place, and the batch totals per arena (one block, tiles of kTotalsThreads
+// blocks). With `out` (mapped host memory) it also publishes the insert plan:
+// out[0..5) totals, out[5] the batch status word, out[6..11) the arena tops.
+__global__ void __launch_bounds__(kTotalsThreads) k_totals(unsigned long long* bsum, uint32_t nb,
+                                                           unsigned long long* tot, const uint32_t* ctl,
+                                                           const unsigned long long* top,
+                                                           volatile unsigned long long* out) {
+  __shared__ unsigned long long wtot[kTotalsThreads / 32][kArenas];
+  __shared__ unsigned long long carry[kArenas];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t < kArenas) carry[t] = 0;
+  for (uint32_t base = 0; base < nb; base += kTotalsThreads) {
+    const uint32_t r = base + (uint32_t)t;
+    unsigned long long x[kArenas], inc[kArenas];
+#pragma unroll
+    for (int a = 0; a < kArenas; ++a) x[a] = r < nb ? bsum[(size_t)a * nb + r] : 0ull;
+#pragma unroll
+    for (int a = 0; a < kArenas; ++a) {
+      inc[a] = x[a];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, inc[a], o);
+        if (lane >= o) inc[a] += y;
+      }
+      if (lane == 31) wtot[w][a] = inc[a];
+      inc[a] -= x[a];  // exclusive within the warp
+    }
+    __syncthreads();
+    if (w == 0) {  // lane v scans warp v's totals, arena by arena
+#pragma unroll
+      for (int a = 0; a < kArenas; ++a) {
+        const unsigned long long y = wtot[lane][a];
+        unsigned long long yi = y;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned long long z = __shfl_up_sync(kFull, yi, o);
+          if (lane >= o) yi += z;
+        }
+        const unsigned long long c0 = carry[a];
+        wtot[lane][a] = c0 + yi - y;
+        const unsigned long long total = __shfl_sync(kFull, yi, 31);
+        __syncwarp();
+        if (lane == 0) carry[a] = c0 + total;
+      }
+    }
+    __syncthreads();
+    if (r < nb) {
+#pragma unroll
+      for (int a = 0; a < kArenas; ++a) bsum[(size_t)a * nb + r] = wtot[w][a] + inc[a];
+    }
+    __syncthreads();  // wtot and carry are reused by the next tile
+  }
+  __syncthreads();
+  if (t < kArenas) tot[t] = carry[t];
+  if (!out || t > kArenas) return;
+  if (t < kArenas) {
+    out[t] = carry[t];
+    out[kArenas + 1 + t] = top[t];
+  } else {
+    out[kArenas] = *ctl;
+  }
+  __threadfence_system();  // only the writers of the host-visible plan
 }
 
 // All-or-nothing reservation of the batch's arena space.
@@ -175,21 +242,21 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
                                                          const uint32_t* sw, const uint32_t* sorig,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, uint32_t ks, const uint32_t* ctl,
-                                                         const ArenaNeed* scan,
+                                                         const ArenaNeed* excl, const unsigned long long* boff,
                                                          const unsigned long long* base, uint32_t* out_slots) {
   __shared__ AliasScratch asc[kBlock / 32];
   if (*ctl) return;
   const uint32_t warps = gridDim.x * blockDim.x / 32;
-  const uint32_t nS = *nseg;
+  const uint32_t nS = *nseg, nb = plan_blocks(ks);
   for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
     uint32_t b, e;
     seg_bounds(seg, nS, s, k, &b, &e);
     const uint32_t u = skey[b];
     if (u >= S.n) continue;
-    const ArenaNeed off = scan[s];
+    const ArenaNeed off = excl[s];
     unsigned long long res[kArenas];
 #pragma unroll
-    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + off.v[a];
+    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + boff[(size_t)a * nb + s / kPlanSegs] + off.v[a];
     apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res, &asc[threadIdx.x / 32]);
   }
 }
@@ -704,8 +771,8 @@ void Engine::ensure_batch_scratch(uint64_t k) {
   nseg_.ensure(16, "scratch");
   ctl_.ensure(16, "scratch");
   base_.ensure(kArenas * 8 * 2, "scratch");
-  need_.ensure((size_t)ks * sizeof(ArenaNeed), "scratch");
-  scan_.ensure((size_t)ks * sizeof(ArenaNeed), "scratch");
+  need_.ensure((size_t)plan_blocks((uint32_t)ks) * sizeof(ArenaNeed), "scratch");  // plan-block sums
+  scan_.ensure((size_t)ks * sizeof(ArenaNeed), "scratch");                                   // in-block offsets
   if (iota_n_ < kk) {
     iota_.ensure(kk * 4, "scratch");
     k_iota<<<grid_for(kk, kBlock), kBlock, 0, stream_>>>(iota_.as<uint32_t>(), kk);
@@ -713,14 +780,12 @@ void Engine::ensure_batch_scratch(uint64_t k) {
     ++launches_;
     iota_n_ = kk;
   }
-  size_t t_sort = 0, t_sel = 0, t_scan = 0;
+  size_t t_sort = 0, t_sel = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const uint32_t*)nullptr, (uint32_t*)nullptr,
                                   (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)kk, 0, 32, stream_);
   cub::DeviceSelect::Flagged(nullptr, t_sel, (const uint32_t*)nullptr, (const uint8_t*)nullptr, (uint32_t*)nullptr,
                              (uint32_t*)nullptr, (int)kk, stream_);
-  cub::DeviceScan::ExclusiveScan(nullptr, t_scan, (const ArenaNeed*)nullptr, (ArenaNeed*)nullptr, AddNeed(),
-                                 ArenaNeed{}, (int)ks, stream_);
-  cub_tmp_.ensure(std::max(t_sort, std::max(t_sel, t_scan)), "scratch");
+  cub_tmp_.ensure(std::max(t_sort, t_sel), "scratch");
   group_cluster_ok();  // probed here, outside any stream capture
 }
 
@@ -734,34 +799,71 @@ const uint32_t* Engine::stage(const uint32_t* p, uint64_t k, DevBuf& buf, const 
 // Stable sort of the batch by vertex; leaves sorted keys in key_s_, the
 // original index in perm_, payloads a/b in sorted order in sa_/sb_, and the
 // segment start list in seg_ with its count in nseg_.
-bool Engine::group_cluster_ok() {
+namespace {
+void group_launch_config(cudaLaunchConfig_t& lc, cudaLaunchAttribute* at, int ctas, uint32_t ipt, cudaStream_t s) {
+  lc = cudaLaunchConfig_t{};
+  lc.gridDim = dim3(ctas);
+  lc.blockDim = dim3(kGroupThreads);
+  lc.dynamicSmemBytes = group_smem_bytes(ipt);
+  lc.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = ctas;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+}
+
+// The grouping kernel for CTAS-CTA clusters can be resident on this device.
+template <int CTAS, int IPT>
+bool group_kernel_ready() {
+  auto kern = k_group_small<CTAS, IPT>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem_bytes(IPT)) !=
+      cudaSuccess)
+    return false;
+  if (CTAS > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return false;
+  cudaLaunchConfig_t lc;
+  cudaLaunchAttribute at[1];
+  group_launch_config(lc, at, CTAS, IPT, nullptr);
+  int clusters = 0;
+  return cudaOccupancyMaxActiveClusters(&clusters, kern, &lc) == cudaSuccess && clusters > 0;
+}
+
+template <int CTAS, int IPT>
+cudaError_t launch_group(cudaStream_t s, const uint32_t* key, const uint32_t* a, const uint32_t* b, uint32_t k,
+                         uint32_t n, int end_bit, bool insert, uint32_t* key_s, uint32_t* perm, uint32_t* sa,
+                         uint32_t* sb, uint32_t* seg, uint32_t* nseg, uint32_t* ctl, uint32_t* err) {
+  const uint32_t ipt = group_ipt(k, CTAS);
+  cudaLaunchConfig_t lc;
+  cudaLaunchAttribute at[1];
+  group_launch_config(lc, at, CTAS, ipt, s);
+  return cudaLaunchKernelEx(&lc, k_group_small<CTAS, IPT>, key, a, b, k, n, end_bit, ipt, insert ? 1 : 0, key_s,
+                            perm, sa, sb, seg, nseg, ctl, err);
+}
+}  // namespace
+
+// Bit 0: 8-CTA grouping clusters can run; bit 1: 16-CTA ones.
+int Engine::group_cluster_ok() {
   if (group_cluster_ < 0) {
-    group_cluster_ = 0;
-    if (cudaFuncSetAttribute(k_group_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)group_smem_bytes(kGroupIpt)) == cudaSuccess) {
-      cudaLaunchConfig_t lc = {};
-      lc.gridDim = dim3(kGroupCtas);
-      lc.blockDim = dim3(kGroupThreads);
-      lc.dynamicSmemBytes = group_smem_bytes(kGroupIpt);
-      int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, k_group_small, &lc) == cudaSuccess && clusters > 0)
-        group_cluster_ = 1;
-    }
+    group_cluster_ = (group_kernel_ready<8, kGroupIptSmall>() ? 1 : 0) |
+                     (group_kernel_ready<16, kGroupIptLarge>() ? 2 : 0);
     cudaGetLastError();  // a refused query leaves the CUB path in place, not a sticky error
   }
-  return group_cluster_ == 1;
+  return group_cluster_;
 }
 
 void Engine::group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k, bool insert) {
   int end_bit = 1;
   while (end_bit < 32 && (1ull << end_bit) < n_) ++end_bit;
-  if (k >= 1 && k <= kGroupMax && group_cluster_ok()) {
-    const uint32_t ipt = group_ipt(k);
-    k_group_small<<<kGroupCtas, kGroupThreads, group_smem_bytes(ipt), stream_>>>(
-        key, a, b, (uint32_t)k, n_, end_bit, ipt, insert ? 1 : 0, key_s_.as<uint32_t>(), perm_.as<uint32_t>(),
-        sa_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), ctl_.as<uint32_t>(),
-        d_err_);
-    cuda_check(cudaGetLastError(), "group batch");
+  const int gc = k >= 1 && k <= kGroupMax ? group_cluster_ok() : 0;
+  const bool small = (gc & 1) && (k <= kGroupSmallMax || (!(gc & 2) && k <= 8ull * kGroupThreads * kGroupIptSmall));
+  if (small || (gc & 2)) {
+    auto* launch = small ? launch_group<8, kGroupIptSmall> : launch_group<16, kGroupIptLarge>;
+    cuda_check(launch(stream_, key, a, b, (uint32_t)k, n_, end_bit, insert, key_s_.as<uint32_t>(),
+                      perm_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(),
+                      nseg_.as<uint32_t>(), ctl_.as<uint32_t>(), d_err_),
+               "group batch");
     ++launches_;
     return;
   }
@@ -852,23 +954,21 @@ void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
   ++arena_gen_;
 }
 
-// Per-segment arena needs of the grouped insert batch, their exclusive scan
-// (each segment's offsets in every arena) and the batch totals, which it
-// returns (device memory); publish != null also writes the insert plan there.
+// Per-segment arena offsets of the grouped insert batch relative to the
+// batch's base (excl in scan_, block prefixes in need_) and the batch totals,
+// which it returns (device memory); publish != null also writes the insert
+// plan there.
 unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t ks,
                                        volatile unsigned long long* publish) {
-  k_plan<<<grid_for((unsigned long long)ks * 32, kBlock, 16), kBlock, 0, stream_>>>(
-      S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks,
-      ctl_.as<uint32_t>(), need_.as<ArenaNeed>());
+  const uint32_t nb = plan_blocks(ks);
+  k_plan<<<nb, kPlanThreads, 0, stream_>>>(S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(),
+                                           nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
+                                           need_.as<unsigned long long>());
   cuda_check(cudaGetLastError(), "plan");
   ++launches_;
-  size_t tb = cub_tmp_.bytes;
-  cuda_check(cub::DeviceScan::ExclusiveScan(cub_tmp_.p, tb, need_.as<ArenaNeed>(), scan_.as<ArenaNeed>(), AddNeed(),
-                                            ArenaNeed{}, (int)ks, stream_),
-             "scan");
   unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
-  k_totals<<<1, 32, 0, stream_>>>(need_.as<ArenaNeed>(), scan_.as<ArenaNeed>(), ks, d_tot, ctl_.as<uint32_t>(),
-                                  d_top_, publish);
+  k_totals<<<1, kTotalsThreads, 0, stream_>>>(need_.as<unsigned long long>(), nb, d_tot, ctl_.as<uint32_t>(), d_top_,
+                                              publish);
   cuda_check(cudaGetLastError(), "totals");
   ++launches_;
   return d_tot;
@@ -903,7 +1003,7 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   ++launches_;
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
       base_.as<unsigned long long>(), dev_out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
@@ -1404,7 +1504,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   ++launches_;
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
+      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
       base_.as<unsigned long long>(), out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;

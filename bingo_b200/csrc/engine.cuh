@@ -152,7 +152,7 @@ class Engine {
   DevBuf fw_in_, fw_fixed_;                   // float weights: staged input, 16.16 fixed point
   DevBuf check_buf_, check_big_;              // store check: totals, large-vertex list
   uint64_t iota_n_ = 0;
-  int group_cluster_ = -1;  // -1 not yet probed, 0 unavailable, 1 available
+  int group_cluster_ = -1;  // -1 not yet probed, else the group_cluster_ok() bits
   // walk scratch
   DevBuf jobs_, prefix_, queue_, wstart_;
   // Host-bound walk outputs: two device staging buffers used in turn; each
@@ -180,7 +180,7 @@ class Engine {
   // with the batch status word zeroed and the batch validated (`insert`: the
   // destinations too, and the weights are nonzero).
   void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k, bool insert);
-  bool group_cluster_ok();  // the one-cluster grouping kernel can run on this device
+  int group_cluster_ok();  // which cluster sizes of the grouping kernel can run here (bit 0: 8, bit 1: 16)
   void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
   unsigned long long* plan_needs(const StoreView& S, uint64_t k, uint32_t ks, volatile unsigned long long* publish);
   void enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k, uint32_t* out_slots);
