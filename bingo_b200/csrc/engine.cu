@@ -4,7 +4,8 @@
 // cluster kernel that validates, sorts stably and lists the segments; larger
 // ones: validate -> CUB radix sort -> gather + segment heads -> segment
 // select) -> plan (per-vertex growth sizes, prefix inside each plan block) ->
-// prefix of the plan-block sums -> reserve -> apply (warp per vertex). Arena
+// prefix of the plan-block sums -> reserve (host, or device without a host
+// synchronisation) -> apply (warp per vertex). Arena
 // offsets come from these prefix sums in segment order, so the
 // layout is a deterministic function of the inputs; arenas are
 // index-addressed and grow by reallocation on the host before a batch that
@@ -157,8 +158,9 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan(StoreView S, const uint32
 
 // Exclusive prefix of the nb plan-block sums (column-major per arena), in
 // place, and the batch totals per arena (one block, tiles of kTotalsThreads
-// blocks). With `out` (mapped host memory) it also publishes the insert plan:
-// out[0..5) totals, out[5] the batch status word, out[6..11) the arena tops.
+// blocks). With `out` (mapped host memory) it also publishes the insert plan,
+// read by the host after a stream synchronize: out[0..5) totals, out[5] the
+// batch status word, out[6..11) the arena tops.
 __global__ void __launch_bounds__(kTotalsThreads) k_totals(unsigned long long* bsum, uint32_t nb,
                                                            unsigned long long* tot, const uint32_t* ctl,
                                                            const unsigned long long* top,
@@ -217,10 +219,17 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(unsigned long long* b
   } else {
     out[kArenas] = *ctl;
   }
-  __threadfence_system();  // only the writers of the host-visible plan
 }
 
-// All-or-nothing reservation of the batch's arena space.
+// Arena bases of a batch reserved by the host (plain inserts, after the plan
+// was read back and the arenas grown): the apply kernel uses them and moves
+// the device tops to `top`.
+struct HostReserve {
+  unsigned long long base[kArenas], top[kArenas];
+};
+
+// All-or-nothing reservation of the batch's arena space on the device
+// (inserts without host synchronisation).
 
 __global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base) {
   if (threadIdx.x || blockIdx.x || *ctl) return;
@@ -243,9 +252,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, uint32_t ks, const uint32_t* ctl,
                                                          const ArenaNeed* excl, const unsigned long long* boff,
-                                                         const unsigned long long* base, uint32_t* out_slots) {
+                                                         const unsigned long long* base, HostReserve hr,
+                                                         uint32_t* out_slots) {
   __shared__ AliasScratch asc[kBlock / 32];
   if (*ctl) return;
+  if (!base && blockIdx.x == 0 && threadIdx.x < kArenas) S.top[threadIdx.x] = hr.top[threadIdx.x];
   const uint32_t warps = gridDim.x * blockDim.x / 32;
   const uint32_t nS = *nseg, nb = plan_blocks(ks);
   for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
@@ -256,7 +267,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
     const ArenaNeed off = excl[s];
     unsigned long long res[kArenas];
 #pragma unroll
-    for (int a = 0; a < kArenas; ++a) res[a] = base[a] + boff[(size_t)a * nb + s / kPlanSegs] + off.v[a];
+    for (int a = 0; a < kArenas; ++a)
+      res[a] = (base ? base[a] : hr.base[a]) + boff[(size_t)a * nb + s / kPlanSegs] + off.v[a];
     apply_append(S, u, sv + b, sw + b, sorig + b, e - b, out_slots, res, &asc[threadIdx.x / 32]);
   }
 }
@@ -998,13 +1010,12 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
       if (h_top_[a] + tot[a] > cap_[a]) grow_arena(a, h_top_[a] + tot[a]);
   }
   const StoreView S = view();
-  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
-  cuda_check(cudaGetLastError(), "reserve");
-  ++launches_;
+  HostReserve hr;  // the plan left the stream idle, so the bases are the tops read with it
+  for (int a = 0; a < kArenas; ++a) hr.base[a] = h_top_[a], hr.top[a] = h_top_[a] + tot[a];
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
       nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
-      base_.as<unsigned long long>(), dev_out_slots);
+      nullptr, hr, dev_out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
   for (int a = 0; a < kArenas; ++a) h_top_[a] += tot[a];
@@ -1505,7 +1516,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
       nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
-      base_.as<unsigned long long>(), out_slots);
+      base_.as<unsigned long long>(), HostReserve{}, out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
 }

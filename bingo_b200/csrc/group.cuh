@@ -85,6 +85,12 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     for (int i = 0; i < IPT_MAX; ++i) {
       const uint32_t g = c * chunk + i * kGroupThreads + t;
       kv[i] = (i < (int)ipt && g < k) ? key[g] : 0xFFFFFFFFu;
+      // The payload is gathered by batch index after the sort: bring the
+      // 128-byte lines this warp's positions cover into L2 now.
+      if (i < (int)ipt && g < k && (l == 0 || l == 31)) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a + g));
+        if (b) asm volatile("prefetch.global.L2 [%0];" ::"l"(b + g));
+      }
     }
 #pragma unroll
     for (int i = 0; i < IPT_MAX; ++i)
