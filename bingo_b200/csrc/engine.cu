@@ -228,23 +228,34 @@ struct HostReserve {
   unsigned long long base[kArenas], top[kArenas];
 };
 
-// All-or-nothing reservation of the batch's arena space on the device
-// (inserts without host synchronisation).
+// All-or-nothing reservation of the batch's arena space on the device. Plain
+// inserts publish the outcome to the host (status) and keep a full arena out
+// of the sticky error word: the host grows the arena and applies the batch
+// again; inserts inside programs raise E_CAPACITY.
+constexpr unsigned long long kReserveOk = 1, kReserveFull = 2, kReserveRejected = 3;
+constexpr int kPlanStatusSlot = 2 * kArenas + 1;  // after totals, status word and tops in the published plan
 
-__global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base) {
-  if (threadIdx.x || blockIdx.x || *ctl) return;
+__global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base,
+                          int sticky, volatile unsigned long long* status) {
+  if (threadIdx.x || blockIdx.x) return;
+  if (*ctl) {
+    if (status) *status = kReserveRejected;
+    return;
+  }
   bool ok = true;
   for (int a = 0; a < kArenas; ++a)
     if (S.top[a] + tot[a] > S.cap[a]) ok = false;
   if (!ok) {
     atomicOr(ctl, E_CAPACITY);
-    atomicOr(S.err, E_CAPACITY);
+    if (sticky) atomicOr(S.err, E_CAPACITY);
+    if (status) *status = kReserveFull;
     return;
   }
   for (int a = 0; a < kArenas; ++a) {
     base[a] = S.top[a];
     S.top[a] += tot[a];
   }
+  if (status) *status = kReserveOk;
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const uint32_t* skey, const uint32_t* sv,
@@ -673,6 +684,7 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
              "cudaHostAlloc(plan)");
   cuda_check(cudaHostGetDevicePointer((void**)&d_plan_, (void*)h_plan_, 0), "plan mapping");
   cuda_check(cudaEventCreateWithFlags(&slots_ev_, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&reserve_ev_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Engine::~Engine() {
@@ -693,6 +705,7 @@ Engine::~Engine() {
   }
   if (xstream_) cudaStreamDestroy(xstream_);
   if (slots_ev_) cudaEventDestroy(slots_ev_);
+  if (reserve_ev_) cudaEventDestroy(reserve_ev_);
   if (h_plan_) cudaFreeHost((void*)h_plan_);
   for (auto& a : arena_) a.release();
   if (d_err_) cudaFree(d_err_);
@@ -988,36 +1001,60 @@ unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t 
 
 // Plan, size, reserve and apply an append batch whose grouped columns are in
 // key_s_/sa_ (dst)/sb_ (w)/perm_ (original index) and segments in seg_/nseg_.
+// A load sizes the arenas from the plan it reads back. An insert reserves on
+// the device and launches the apply kernel at once; the host then waits only
+// for the reservation (the apply kernel runs meanwhile) and, when an arena
+// was full (the apply kernel skipped the batch), grows it and applies the
+// batch again before returning, so later work always sees the batch applied.
 void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t) {
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   const StoreView S0 = view();
   unsigned long long* d_tot = plan_needs(S0, k, ks, d_plan_);
-  cuda_check(cudaStreamSynchronize(stream_), "plan sync");
+  auto apply = [&](const StoreView& S, const unsigned long long* dev_base, const HostReserve& hr) {
+    k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0,
+                     stream_>>>(S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(),
+                                seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(),
+                                scan_.as<ArenaNeed>(), need_.as<unsigned long long>(), dev_base, hr, dev_out_slots);
+    cuda_check(cudaGetLastError(), "apply insert");
+    ++launches_;
+  };
+  if (!load_mode) {
+    k_reserve<<<1, 1, 0, stream_>>>(S0, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>(), 0,
+                                    d_plan_ + kPlanStatusSlot);
+    cuda_check(cudaGetLastError(), "reserve");
+    ++launches_;
+    cuda_check(cudaEventRecord(reserve_ev_, stream_), "reserve");
+    apply(S0, base_.as<unsigned long long>(), HostReserve{});
+    cuda_check(cudaEventSynchronize(reserve_ev_), "plan sync");
+  } else {
+    cuda_check(cudaStreamSynchronize(stream_), "plan sync");
+  }
   unsigned long long tot[kArenas];
   for (int a = 0; a < kArenas; ++a) tot[a] = h_plan_[a];
   const uint32_t ctl = (uint32_t)h_plan_[kArenas];
   if (!load_mode)
     for (int a = 0; a < kArenas; ++a) h_top_[a] = h_plan_[kArenas + 1 + a];
   if (ctl) {
+    cuda_check(cudaStreamSynchronize(stream_), "rejected batch");
     cuda_check(cudaMemset(d_err_, 0, 2 * sizeof(uint32_t)), "clear status");
     const int st = status_of(ctl);
     throw Error(st, st == BINGO_ERR_ZERO_WEIGHT ? "batch holds a zero weight" : "batch holds a vertex id >= n");
   }
   if (load_mode) {
     alloc_arenas(tot);
-  } else {
+    HostReserve hr;
+    for (int a = 0; a < kArenas; ++a) hr.base[a] = h_top_[a], hr.top[a] = h_top_[a] + tot[a];
+    apply(view(), nullptr, hr);
+  } else if (h_plan_[kPlanStatusSlot] != kReserveOk) {
+    // An arena was full: nothing was applied. Grow, clear the status word and
+    // apply with bases from the host.
     for (int a = 0; a < kArenas; ++a)
       if (h_top_[a] + tot[a] > cap_[a]) grow_arena(a, h_top_[a] + tot[a]);
+    cuda_check(cudaMemsetAsync(ctl_.p, 0, 4, stream_), "ctl");
+    HostReserve hr;
+    for (int a = 0; a < kArenas; ++a) hr.base[a] = h_top_[a], hr.top[a] = h_top_[a] + tot[a];
+    apply(view(), nullptr, hr);
   }
-  const StoreView S = view();
-  HostReserve hr;  // the plan left the stream idle, so the bases are the tops read with it
-  for (int a = 0; a < kArenas; ++a) hr.base[a] = h_top_[a], hr.top[a] = h_top_[a] + tot[a];
-  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
-      S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
-      nullptr, hr, dev_out_slots);
-  cuda_check(cudaGetLastError(), "apply insert");
-  ++launches_;
   for (int a = 0; a < kArenas; ++a) h_top_[a] += tot[a];
 }
 
@@ -1510,7 +1547,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   group_by_vertex(a, b, c, k, true);
   const StoreView S = view();
   unsigned long long* d_tot = plan_needs(S, k, ks, nullptr);
-  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>());
+  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>(), 1, nullptr);
   cuda_check(cudaGetLastError(), "reserve");
   ++launches_;
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(

@@ -141,6 +141,7 @@ class Engine {
   volatile unsigned long long* h_plan_ = nullptr;
   unsigned long long* d_plan_ = nullptr;
   cudaEvent_t slots_ev_ = nullptr;  // host-bound slot ids copied out (asynchronous handles)
+  cudaEvent_t reserve_ev_ = nullptr;  // an insert's device reservation is done (its plan is published)
   bool slots_busy_ = false;
   unsigned long long* d_steps_ = nullptr;  // produced walk steps since create
   unsigned long long launches_ = 0;        // hand-written kernels launched since create
