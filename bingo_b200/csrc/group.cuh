@@ -69,6 +69,10 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
   const uint32_t c = cluster.block_rank();
   const uint32_t t = threadIdx.x, w = t >> 5, l = t & 31;
   const uint32_t chunk = ipt * kGroupThreads;  // this CTA owns global positions [c * chunk, (c + 1) * chunk)
+  // __umulhi(pos, cmagic) == pos / chunk for every pos < CTAS * chunk: with
+  // cmagic = ceil(2^32 / chunk) the error is below pos / 2^32 < 2^-15 and
+  // pos % chunk <= chunk - 1 < chunk * (1 - 2^-15) (chunk < 2^15).
+  const uint32_t cmagic = (uint32_t)((0x100000000ull + chunk - 1) / chunk);
   uint2* in = g_items;                         // in[j] holds global position c * chunk + j
   uint2* out = g_items + chunk;
   uint16_t (*cnt)[BINS] = reinterpret_cast<uint16_t (*)[BINS]>(g_items + 2 * chunk);  // per warp and digit
@@ -103,8 +107,8 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
   const uint32_t wbase = w * 32 * ipt;
   for (int shift = 0; shift < end_bit; shift += BITS) {
     const uint32_t mask = end_bit - shift >= BITS ? (uint32_t)BINS - 1 : (1u << (end_bit - shift)) - 1;
-    for (uint32_t x = t; x < kGroupWarps * BINS / 2; x += kGroupThreads)
-      reinterpret_cast<uint32_t*>(&cnt[0][0])[x] = 0;
+    for (uint32_t x = t; x < kGroupWarps * BINS / 8; x += kGroupThreads)
+      reinterpret_cast<uint4*>(&cnt[0][0])[x] = make_uint4(0, 0, 0, 0);
     __syncthreads();
     uint32_t rk[IPT_MAX];
 #pragma unroll
@@ -130,15 +134,18 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
       }
     }
     __syncthreads();
-    {  // per digit (thread t = digit): exclusive prefix over warps, CTA count
+    if (t < BINS / 2) {  // digits 2t and 2t + 1 as one word: exclusive prefix over warps, CTA counts
+      // (a CTA holds at most 8,192 items, so the low half never carries into the high one)
+      uint32_t* cw = reinterpret_cast<uint32_t*>(&cnt[0][0]);
       uint32_t run = 0;
 #pragma unroll
       for (int v = 0; v < kGroupWarps; ++v) {
-        const uint32_t x = cnt[v][t];
-        cnt[v][t] = (uint16_t)run;
+        const uint32_t x = cw[v * (BINS / 2) + t];
+        cw[v * (BINS / 2) + t] = run;
         run += x;
       }
-      hist[t] = run;
+      hist[2 * t] = run & 0xFFFFu;
+      hist[2 * t + 1] = run >> 16;
     }
     cluster.sync();  // every CTA's digit counts are complete
     uint32_t tot = 0, before = 0;
@@ -156,11 +163,18 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     }
     if (l == 31) wsum[w] = inc;
     __syncthreads();
-    {
-      uint32_t p = 0;
-      for (uint32_t v = 0; v < w; ++v) p += wsum[v];
-      gbase[t] = p + inc - tot + before;  // all smaller digits + this digit in lower-ranked CTAs
+    if (w == 0) {  // exclusive prefix of the warp totals
+      const uint32_t x = wsum[l];
+      uint32_t y = x;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t z = __shfl_up_sync(kFull, y, o);
+        if (l >= (uint32_t)o) y += z;
+      }
+      wsum[l] = y - x;
     }
+    __syncthreads();
+    gbase[t] = wsum[w] + inc - tot + before;  // all smaller digits + this digit in lower-ranked CTAs
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < IPT_MAX; ++i) {
@@ -168,7 +182,8 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
         const uint2 v = in[wbase + i * 32 + l];
         const uint32_t d = (v.x >> shift) & mask;
         const uint32_t pos = gbase[d] + cnt[w][d] + rk[i];
-        cluster.map_shared_rank(out, pos / chunk)[pos % chunk] = v;
+        const uint32_t r = __umulhi(pos, cmagic);  // pos / chunk
+        cluster.map_shared_rank(out, r)[pos - r * chunk] = v;
       }
     }
     cluster.sync();  // the pass's scatter has landed everywhere
