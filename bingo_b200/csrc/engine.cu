@@ -4,12 +4,11 @@
 // cluster kernel that validates, sorts stably and lists the segments; larger
 // ones: validate -> CUB radix sort -> gather + segment heads -> segment
 // select) -> plan (per-vertex growth sizes, prefix inside each plan block) ->
-// prefix of the plan-block sums -> reserve (host, or device without a host
-// synchronisation) -> apply (warp per vertex). Arena
-// offsets come from these prefix sums in segment order, so the
-// layout is a deterministic function of the inputs; arenas are
-// index-addressed and grow by reallocation on the host before a batch that
-// would not fit.
+// prefix of the plan-block sums and the batch's arena reservation (one
+// block) -> apply (warp per vertex). Arena offsets come from these prefix
+// sums in segment order, so the layout is a deterministic function of the
+// inputs; arenas are index-addressed and grow by reallocation on the host
+// (before a load, or when a batch did not fit).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -156,14 +155,25 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan(StoreView S, const uint32
   }
 }
 
+// Device reservation modes of k_totals and the outcome it publishes.
+enum ReserveMode { kReserveNone = 0, kReservePublish = 1, kReserveSticky = 2 };
+constexpr unsigned long long kReserveOk = 1, kReserveFull = 2, kReserveRejected = 3;
+constexpr int kPlanStatusSlot = 2 * kArenas + 1;  // after totals, status word and tops in the published plan
+
 // Exclusive prefix of the nb plan-block sums (column-major per arena), in
 // place, and the batch totals per arena (one block, tiles of kTotalsThreads
 // blocks). With `out` (mapped host memory) it also publishes the insert plan,
-// read by the host after a stream synchronize: out[0..5) totals, out[5] the
-// batch status word, out[6..11) the arena tops.
-__global__ void __launch_bounds__(kTotalsThreads) k_totals(unsigned long long* bsum, uint32_t nb,
-                                                           unsigned long long* tot, const uint32_t* ctl,
-                                                           const unsigned long long* top,
+// read by the host after the launch completes: out[0..5) totals, out[5] the
+// batch status word, out[6..11) the arena tops before this batch.
+// `reserve` != kReserveNone then reserves the batch's arena space, all or
+// nothing: base = the tops, tops += totals. A full arena sets E_CAPACITY in
+// the batch status word (the apply kernel then skips the batch); with
+// kReservePublish the outcome goes to out[kPlanStatusSlot] and the host grows
+// the arena and applies the batch again, with kReserveSticky (programs) the
+// error also goes to the sticky error word.
+__global__ void __launch_bounds__(kTotalsThreads) k_totals(StoreView S, unsigned long long* bsum, uint32_t nb,
+                                                           unsigned long long* tot, uint32_t* ctl,
+                                                           unsigned long long* base, int reserve,
                                                            volatile unsigned long long* out) {
   __shared__ unsigned long long wtot[kTotalsThreads / 32][kArenas];
   __shared__ unsigned long long carry[kArenas];
@@ -211,13 +221,41 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(unsigned long long* b
     __syncthreads();  // wtot and carry are reused by the next tile
   }
   __syncthreads();
-  if (t < kArenas) tot[t] = carry[t];
+  unsigned long long top0 = 0;
+  uint32_t ctl0 = 0;
+  if (t < kArenas) {
+    tot[t] = carry[t];
+    top0 = S.top[t];
+  }
+  if (t == kArenas) ctl0 = *ctl;
+  __syncthreads();  // the tops and the status word are read before the reservation changes them
+  if (reserve != kReserveNone && t == 0) {
+    unsigned long long st = kReserveOk;
+    if (*ctl) {
+      st = kReserveRejected;
+    } else {
+      bool ok = true;
+      for (int a = 0; a < kArenas; ++a)
+        if (S.top[a] + carry[a] > S.cap[a]) ok = false;
+      if (ok) {
+        for (int a = 0; a < kArenas; ++a) {
+          base[a] = S.top[a];
+          S.top[a] += carry[a];
+        }
+      } else {
+        st = kReserveFull;
+        atomicOr(ctl, E_CAPACITY);
+        if (reserve == kReserveSticky) atomicOr(S.err, E_CAPACITY);
+      }
+    }
+    if (out) out[kPlanStatusSlot] = st;
+  }
   if (!out || t > kArenas) return;
   if (t < kArenas) {
     out[t] = carry[t];
-    out[kArenas + 1 + t] = top[t];
+    out[kArenas + 1 + t] = top0;
   } else {
-    out[kArenas] = *ctl;
+    out[kArenas] = ctl0;
   }
 }
 
@@ -228,35 +266,7 @@ struct HostReserve {
   unsigned long long base[kArenas], top[kArenas];
 };
 
-// All-or-nothing reservation of the batch's arena space on the device. Plain
-// inserts publish the outcome to the host (status) and keep a full arena out
-// of the sticky error word: the host grows the arena and applies the batch
-// again; inserts inside programs raise E_CAPACITY.
-constexpr unsigned long long kReserveOk = 1, kReserveFull = 2, kReserveRejected = 3;
-constexpr int kPlanStatusSlot = 2 * kArenas + 1;  // after totals, status word and tops in the published plan
 
-__global__ void k_reserve(StoreView S, const unsigned long long* tot, uint32_t* ctl, unsigned long long* base,
-                          int sticky, volatile unsigned long long* status) {
-  if (threadIdx.x || blockIdx.x) return;
-  if (*ctl) {
-    if (status) *status = kReserveRejected;
-    return;
-  }
-  bool ok = true;
-  for (int a = 0; a < kArenas; ++a)
-    if (S.top[a] + tot[a] > S.cap[a]) ok = false;
-  if (!ok) {
-    atomicOr(ctl, E_CAPACITY);
-    if (sticky) atomicOr(S.err, E_CAPACITY);
-    if (status) *status = kReserveFull;
-    return;
-  }
-  for (int a = 0; a < kArenas; ++a) {
-    base[a] = S.top[a];
-    S.top[a] += tot[a];
-  }
-  if (status) *status = kReserveOk;
-}
 
 __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const uint32_t* skey, const uint32_t* sv,
                                                          const uint32_t* sw, const uint32_t* sorig,
@@ -984,7 +994,7 @@ void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
 // which it returns (device memory); publish != null also writes the insert
 // plan there.
 unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t ks,
-                                       volatile unsigned long long* publish) {
+                                       volatile unsigned long long* publish, int reserve) {
   const uint32_t nb = plan_blocks(ks);
   k_plan<<<nb, kPlanThreads, 0, stream_>>>(S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(),
                                            nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
@@ -992,8 +1002,8 @@ unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t 
   cuda_check(cudaGetLastError(), "plan");
   ++launches_;
   unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
-  k_totals<<<1, kTotalsThreads, 0, stream_>>>(need_.as<unsigned long long>(), nb, d_tot, ctl_.as<uint32_t>(), d_top_,
-                                              publish);
+  k_totals<<<1, kTotalsThreads, 0, stream_>>>(S, need_.as<unsigned long long>(), nb, d_tot, ctl_.as<uint32_t>(),
+                                              base_.as<unsigned long long>(), reserve, publish);
   cuda_check(cudaGetLastError(), "totals");
   ++launches_;
   return d_tot;
@@ -1009,7 +1019,7 @@ unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t 
 void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t) {
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   const StoreView S0 = view();
-  unsigned long long* d_tot = plan_needs(S0, k, ks, d_plan_);
+  plan_needs(S0, k, ks, d_plan_, load_mode ? kReserveNone : kReservePublish);
   auto apply = [&](const StoreView& S, const unsigned long long* dev_base, const HostReserve& hr) {
     k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0,
                      stream_>>>(S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(),
@@ -1019,10 +1029,6 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
     ++launches_;
   };
   if (!load_mode) {
-    k_reserve<<<1, 1, 0, stream_>>>(S0, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>(), 0,
-                                    d_plan_ + kPlanStatusSlot);
-    cuda_check(cudaGetLastError(), "reserve");
-    ++launches_;
     cuda_check(cudaEventRecord(reserve_ev_, stream_), "reserve");
     apply(S0, base_.as<unsigned long long>(), HostReserve{});
     cuda_check(cudaEventSynchronize(reserve_ev_), "plan sync");
@@ -1546,10 +1552,7 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   group_by_vertex(a, b, c, k, true);
   const StoreView S = view();
-  unsigned long long* d_tot = plan_needs(S, k, ks, nullptr);
-  k_reserve<<<1, 1, 0, stream_>>>(S, d_tot, ctl_.as<uint32_t>(), base_.as<unsigned long long>(), 1, nullptr);
-  cuda_check(cudaGetLastError(), "reserve");
-  ++launches_;
+  plan_needs(S, k, ks, nullptr, kReserveSticky);
   k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
       S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
       nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),

@@ -183,7 +183,8 @@ class Engine {
   void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k, bool insert);
   int group_cluster_ok();  // which cluster sizes of the grouping kernel can run here (bit 0: 8, bit 1: 16)
   void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
-  unsigned long long* plan_needs(const StoreView& S, uint64_t k, uint32_t ks, volatile unsigned long long* publish);
+  unsigned long long* plan_needs(const StoreView& S, uint64_t k, uint32_t ks, volatile unsigned long long* publish,
+                                 int reserve);
   void enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k, uint32_t* out_slots);
   void enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k);
   void ensure_headroom(uint64_t k_insert_total);
