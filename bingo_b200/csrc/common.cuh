@@ -9,6 +9,15 @@
 namespace bingo {
 
 constexpr unsigned kFull = 0xffffffffu;
+
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while the kernel before it still runs;
+// pdl_wait() (first statement of such a kernel) returns once that kernel has
+// completed and its memory is visible, and is a no-op for a plain launch.
+// pdl_trigger() lets the next kernel be scheduled early (its CTAs then wait
+// in pdl_wait()).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 constexpr int kBits = 32;            // weight bits = possible groups per vertex
 constexpr uint32_t kMinEdgeCap = 16; // reference ORIGINAL (include/api.h:13)
 constexpr uint32_t kMinGroupCap = 4; // member lists are allocated in 16-byte units

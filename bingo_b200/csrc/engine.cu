@@ -59,6 +59,22 @@ unsigned grid_for(unsigned long long items, unsigned per_block, unsigned max_per
   return (unsigned)std::max(1ull, std::min(want, cap));
 }
 
+// Launch with programmatic stream serialization (the kernel starts with
+// pdl_wait()): its scheduling overlaps the end of the kernel before it.
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(grid);
+  lc.blockDim = dim3(block);
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  cuda_check(cudaLaunchKernelEx(&lc, kern, static_cast<KArgs>(args)...), "launch");
+}
+
 // ------------------------------------------------------------------ kernels
 __global__ void k_iota(uint32_t* a, unsigned long long n) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
@@ -122,6 +138,8 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan(StoreView S, const uint32
                                                        const uint32_t* seg, const uint32_t* nseg,
                                                        unsigned long long k, uint32_t ks, const uint32_t* ctl,
                                                        ArenaNeed* excl, unsigned long long* bsum) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ unsigned long long nd_s[kPlanSegs][kArenas];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t s = blockIdx.x * kPlanSegs + w;
@@ -175,6 +193,8 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(StoreView S, unsigned
                                                            unsigned long long* tot, uint32_t* ctl,
                                                            unsigned long long* base, int reserve,
                                                            volatile unsigned long long* out) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ unsigned long long wtot[kTotalsThreads / 32][kArenas];
   __shared__ unsigned long long carry[kArenas];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -275,9 +295,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
                                                          const ArenaNeed* excl, const unsigned long long* boff,
                                                          const unsigned long long* base, HostReserve hr,
                                                          uint32_t* out_slots) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ AliasScratch asc[kBlock / 32];
   if (*ctl) return;
-  if (!base && blockIdx.x == 0 && threadIdx.x < kArenas) S.top[threadIdx.x] = hr.top[threadIdx.x];
+  if (!base && blockIdx.x == 0) {
+#pragma unroll
+    for (int a = 0; a < kArenas; ++a)
+      if (threadIdx.x == a) S.top[a] = hr.top[a];  // constant indices keep hr in parameter space
+  }
   const uint32_t warps = gridDim.x * blockDim.x / 32;
   const uint32_t nS = *nseg, nb = plan_blocks(ks);
   for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nS; s += warps) {
@@ -297,6 +323,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_insert(StoreView S, const u
 __global__ void __launch_bounds__(kBlock, 3) k_apply_delete(StoreView S, const uint32_t* skey, const uint32_t* sslot,
                                                          const uint32_t* seg, const uint32_t* nseg,
                                                          unsigned long long k, const uint32_t* ctl) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ AliasScratch asc[kBlock / 32];
   __shared__ uint32_t stage[kBlock / 32][64];
   if (*ctl) return;
@@ -845,8 +873,10 @@ void group_launch_config(cudaLaunchConfig_t& lc, cudaLaunchAttribute* at, int ct
   at[0].val.clusterDim.x = ctas;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   lc.attrs = at;
-  lc.numAttrs = 1;
+  lc.numAttrs = 2;
 }
 
 // The grouping kernel for CTAS-CTA clusters can be resident on this device.
@@ -859,7 +889,7 @@ bool group_kernel_ready() {
   if (CTAS > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     return false;
   cudaLaunchConfig_t lc;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   group_launch_config(lc, at, CTAS, IPT, nullptr);
   int clusters = 0;
   return cudaOccupancyMaxActiveClusters(&clusters, kern, &lc) == cudaSuccess && clusters > 0;
@@ -871,7 +901,7 @@ cudaError_t launch_group(cudaStream_t s, const uint32_t* key, const uint32_t* a,
                          uint32_t* sb, uint32_t* seg, uint32_t* nseg, uint32_t* ctl, uint32_t* err) {
   const uint32_t ipt = group_ipt(k, CTAS);
   cudaLaunchConfig_t lc;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   group_launch_config(lc, at, CTAS, ipt, s);
   return cudaLaunchKernelEx(&lc, k_group_small<CTAS, IPT>, key, a, b, k, n, end_bit, ipt, insert ? 1 : 0, key_s,
                             perm, sa, sb, seg, nseg, ctl, err);
@@ -996,14 +1026,13 @@ void Engine::alloc_arenas(const unsigned long long need[kArenas]) {
 unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t ks,
                                        volatile unsigned long long* publish, int reserve) {
   const uint32_t nb = plan_blocks(ks);
-  k_plan<<<nb, kPlanThreads, 0, stream_>>>(S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(),
-                                           nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
-                                           need_.as<unsigned long long>());
+  launch_pdl(k_plan, nb, kPlanThreads, stream_, S, key_s_.as<uint32_t>(), sb_.as<uint32_t>(), seg_.as<uint32_t>(),
+             nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>());
   cuda_check(cudaGetLastError(), "plan");
   ++launches_;
   unsigned long long* d_tot = base_.as<unsigned long long>() + kArenas;
-  k_totals<<<1, kTotalsThreads, 0, stream_>>>(S, need_.as<unsigned long long>(), nb, d_tot, ctl_.as<uint32_t>(),
-                                              base_.as<unsigned long long>(), reserve, publish);
+  launch_pdl(k_totals, 1, kTotalsThreads, stream_, S, need_.as<unsigned long long>(), nb, d_tot, ctl_.as<uint32_t>(),
+             base_.as<unsigned long long>(), reserve, publish);
   cuda_check(cudaGetLastError(), "totals");
   ++launches_;
   return d_tot;
@@ -1021,10 +1050,10 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
   const StoreView S0 = view();
   plan_needs(S0, k, ks, d_plan_, load_mode ? kReserveNone : kReservePublish);
   auto apply = [&](const StoreView& S, const unsigned long long* dev_base, const HostReserve& hr) {
-    k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0,
-                     stream_>>>(S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(),
-                                seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(),
-                                scan_.as<ArenaNeed>(), need_.as<unsigned long long>(), dev_base, hr, dev_out_slots);
+    launch_pdl(k_apply_insert, grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock,
+               stream_, S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(),
+               seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
+               need_.as<unsigned long long>(), dev_base, hr, dev_out_slots);
     cuda_check(cudaGetLastError(), "apply insert");
     ++launches_;
   };
@@ -1261,9 +1290,9 @@ void Engine::erase_one(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   const uint32_t* dsl = stage(slot, k, in_b_, "stage slot");
   group_by_vertex(du, dsl, nullptr, k, false);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
-  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
-      view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
-      ctl_.as<uint32_t>());
+  launch_pdl(k_apply_delete, grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock,
+             stream_, view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
+             ctl_.as<uint32_t>());
   cuda_check(cudaGetLastError(), "apply delete");
   ++launches_;
 }
@@ -1553,10 +1582,10 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
   group_by_vertex(a, b, c, k, true);
   const StoreView S = view();
   plan_needs(S, k, ks, nullptr, kReserveSticky);
-  k_apply_insert<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
-      S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(), seg_.as<uint32_t>(),
-      nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(), need_.as<unsigned long long>(),
-      base_.as<unsigned long long>(), HostReserve{}, out_slots);
+  launch_pdl(k_apply_insert, grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock,
+             stream_, S, key_s_.as<uint32_t>(), sa_.as<uint32_t>(), sb_.as<uint32_t>(), perm_.as<uint32_t>(),
+             seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k, ks, ctl_.as<uint32_t>(), scan_.as<ArenaNeed>(),
+             need_.as<unsigned long long>(), base_.as<unsigned long long>(), HostReserve{}, out_slots);
   cuda_check(cudaGetLastError(), "apply insert");
   ++launches_;
 }
@@ -1564,9 +1593,9 @@ void Engine::enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t
 void Engine::enqueue_delete(const uint32_t* u, const uint32_t* slot, uint64_t k) {
   group_by_vertex(u, slot, nullptr, k, false);
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
-  k_apply_delete<<<grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock, 0, stream_>>>(
-      view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
-      ctl_.as<uint32_t>());
+  launch_pdl(k_apply_delete, grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock,
+             stream_, view(), key_s_.as<uint32_t>(), sa_.as<uint32_t>(), seg_.as<uint32_t>(), nseg_.as<uint32_t>(), k,
+             ctl_.as<uint32_t>());
   cuda_check(cudaGetLastError(), "apply delete");
   ++launches_;
 }

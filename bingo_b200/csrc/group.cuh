@@ -77,6 +77,8 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
   uint2* out = g_items + chunk;
   uint16_t (*cnt)[BINS] = reinterpret_cast<uint16_t (*)[BINS]>(g_items + 2 * chunk);  // per warp and digit
 
+  pdl_wait();  // launched with programmatic serialization: the batch and ctl are ready after this
+  pdl_trigger();
   if (c == 0 && t < 4) {
     ctl[t] = 0;
     __threadfence();
