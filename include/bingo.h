@@ -134,7 +134,12 @@ int bingo_load_edges(bingo_handle* h, const uint32_t* src, const uint32_t* dst, 
  * (include/operation.cuh:144). Edges append to their source in batch order
  * (the stable_sort of include/operation.cuh:147). out_slots (may be NULL)
  * receives each edge's slot id, the id the reference caller tracks as d[u]++
- * (include/graph.cuh:66) and later passes to delete. Weight 0 is rejected. */
+ * (include/graph.cuh:66) and later passes to delete. Weight 0 is rejected.
+ * The call waits on the host until the batch is validated and its arena
+ * space reserved (the apply kernel already runs meanwhile; a batch that did
+ * not fit is applied again after the arenas grow), so even on an
+ * asynchronous handle a rejected batch is reported by this call, with
+ * nothing applied. */
 int bingo_insert_batch(bingo_handle* h, const uint32_t* src, const uint32_t* dst, const uint32_t* w, uint64_t k,
                        uint32_t* out_slots);
 
