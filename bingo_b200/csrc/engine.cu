@@ -12,6 +12,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -179,10 +181,11 @@ constexpr unsigned long long kReserveOk = 1, kReserveFull = 2, kReserveRejected 
 constexpr int kPlanStatusSlot = 2 * kArenas + 1;  // after totals, status word and tops in the published plan
 
 // Exclusive prefix of the nb plan-block sums (column-major per arena), in
-// place, and the batch totals per arena (one block, tiles of kTotalsThreads
-// blocks). With `out` (mapped host memory) it also publishes the insert plan,
-// read by the host after the launch completes: out[0..5) totals, out[5] the
-// batch status word, out[6..11) the arena tops before this batch.
+// place, and the batch totals per arena (one block; two tiles of
+// kTotalsThreads block sums per barrier pass). With `out` (mapped host memory) it also publishes the insert plan,
+// out[0..5) totals, out[5] the batch status word, out[6..11) the arena tops
+// before this batch, and last (after a system fence) out[kPlanStatusSlot],
+// nonzero once the rest is visible to the host.
 // `reserve` != kReserveNone then reserves the batch's arena space, all or
 // nothing: base = the tops, tops += totals. A full arena sets E_CAPACITY in
 // the batch status word (the apply kernel then skips the batch); with
@@ -195,50 +198,63 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(StoreView S, unsigned
                                                            volatile unsigned long long* out) {
   pdl_wait();
   pdl_trigger();
-  __shared__ unsigned long long wtot[kTotalsThreads / 32][kArenas];
+  constexpr int kTiles = 2;  // tiles of kTotalsThreads block sums scanned per barrier pass
+  __shared__ unsigned long long wtot[kTiles][kTotalsThreads / 32][kArenas];
   __shared__ unsigned long long carry[kArenas];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   if (t < kArenas) carry[t] = 0;
-  for (uint32_t base = 0; base < nb; base += kTotalsThreads) {
-    const uint32_t r = base + (uint32_t)t;
-    unsigned long long x[kArenas], inc[kArenas];
+  for (uint32_t base = 0; base < nb; base += kTiles * kTotalsThreads) {
+    unsigned long long x[kTiles][kArenas], inc[kTiles][kArenas];
 #pragma unroll
-    for (int a = 0; a < kArenas; ++a) x[a] = r < nb ? bsum[(size_t)a * nb + r] : 0ull;
+    for (int q = 0; q < kTiles; ++q) {
+      const uint32_t r = base + (uint32_t)(q * kTotalsThreads + t);
 #pragma unroll
-    for (int a = 0; a < kArenas; ++a) {
-      inc[a] = x[a];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(kFull, inc[a], o);
-        if (lane >= o) inc[a] += y;
-      }
-      if (lane == 31) wtot[w][a] = inc[a];
-      inc[a] -= x[a];  // exclusive within the warp
+      for (int a = 0; a < kArenas; ++a) x[q][a] = r < nb ? bsum[(size_t)a * nb + r] : 0ull;
     }
-    __syncthreads();
-    if (w == 0) {  // lane v scans warp v's totals, arena by arena
+#pragma unroll
+    for (int q = 0; q < kTiles; ++q)
 #pragma unroll
       for (int a = 0; a < kArenas; ++a) {
-        const unsigned long long y = wtot[lane][a];
-        unsigned long long yi = y;
+        inc[q][a] = x[q][a];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const unsigned long long z = __shfl_up_sync(kFull, yi, o);
-          if (lane >= o) yi += z;
+          const unsigned long long y = __shfl_up_sync(kFull, inc[q][a], o);
+          if (lane >= o) inc[q][a] += y;
         }
-        const unsigned long long c0 = carry[a];
-        wtot[lane][a] = c0 + yi - y;
-        const unsigned long long total = __shfl_sync(kFull, yi, 31);
+        if (lane == 31) wtot[q][w][a] = inc[q][a];
+        inc[q][a] -= x[q][a];  // exclusive within the warp
+      }
+    __syncthreads();
+    if (w == 0) {  // lane v scans warp v's totals, tile by tile and arena by arena
+#pragma unroll
+      for (int a = 0; a < kArenas; ++a) {
+        unsigned long long run = carry[a];
+#pragma unroll
+        for (int q = 0; q < kTiles; ++q) {
+          const unsigned long long y = wtot[q][lane][a];
+          unsigned long long yi = y;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long z = __shfl_up_sync(kFull, yi, o);
+            if (lane >= o) yi += z;
+          }
+          wtot[q][lane][a] = run + yi - y;
+          run += __shfl_sync(kFull, yi, 31);
+        }
         __syncwarp();
-        if (lane == 0) carry[a] = c0 + total;
+        if (lane == 0) carry[a] = run;
       }
     }
     __syncthreads();
-    if (r < nb) {
 #pragma unroll
-      for (int a = 0; a < kArenas; ++a) bsum[(size_t)a * nb + r] = wtot[w][a] + inc[a];
+    for (int q = 0; q < kTiles; ++q) {
+      const uint32_t r = base + (uint32_t)(q * kTotalsThreads + t);
+      if (r < nb) {
+#pragma unroll
+        for (int a = 0; a < kArenas; ++a) bsum[(size_t)a * nb + r] = wtot[q][w][a] + inc[q][a];
+      }
     }
-    __syncthreads();  // wtot and carry are reused by the next tile
+    __syncthreads();  // wtot and carry are reused by the next pass
   }
   __syncthreads();
   unsigned long long top0 = 0;
@@ -249,6 +265,7 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(StoreView S, unsigned
   }
   if (t == kArenas) ctl0 = *ctl;
   __syncthreads();  // the tops and the status word are read before the reservation changes them
+  __shared__ unsigned long long status;
   if (reserve != kReserveNone && t == 0) {
     unsigned long long st = kReserveOk;
     if (*ctl) {
@@ -268,15 +285,19 @@ __global__ void __launch_bounds__(kTotalsThreads) k_totals(StoreView S, unsigned
         if (reserve == kReserveSticky) atomicOr(S.err, E_CAPACITY);
       }
     }
-    if (out) out[kPlanStatusSlot] = st;
+    status = st;
   }
-  if (!out || t > kArenas) return;
+  if (!out) return;
   if (t < kArenas) {
     out[t] = carry[t];
     out[kArenas + 1 + t] = top0;
-  } else {
+  } else if (t == kArenas) {
     out[kArenas] = ctl0;
   }
+  if (t <= kArenas) __threadfence_system();
+  __syncthreads();
+  // The status word goes last: a host that sees it nonzero sees the plan.
+  if (t == 0) out[kPlanStatusSlot] = reserve != kReserveNone ? status : kReserveOk;
 }
 
 // Arena bases of a batch reserved by the host (plain inserts, after the plan
@@ -722,7 +743,6 @@ Engine::Engine(const bingo_config& cfg) : cfg_(cfg) {
              "cudaHostAlloc(plan)");
   cuda_check(cudaHostGetDevicePointer((void**)&d_plan_, (void*)h_plan_, 0), "plan mapping");
   cuda_check(cudaEventCreateWithFlags(&slots_ev_, cudaEventDisableTiming), "cudaEventCreate");
-  cuda_check(cudaEventCreateWithFlags(&reserve_ev_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Engine::~Engine() {
@@ -743,7 +763,6 @@ Engine::~Engine() {
   }
   if (xstream_) cudaStreamDestroy(xstream_);
   if (slots_ev_) cudaEventDestroy(slots_ev_);
-  if (reserve_ev_) cudaEventDestroy(reserve_ev_);
   if (h_plan_) cudaFreeHost((void*)h_plan_);
   for (auto& a : arena_) a.release();
   if (d_err_) cudaFree(d_err_);
@@ -1038,6 +1057,24 @@ unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t 
   return d_tot;
 }
 
+// Waits until k_totals has published the insert plan (its status word turns
+// nonzero), with the apply kernel already enqueued behind it so the stream
+// is never drained here. Bounded: after kPlanWaitSeconds the stream is
+// synchronised instead (which also surfaces a device fault).
+void Engine::wait_plan() {
+  constexpr double kPlanWaitSeconds = 5.0;
+  const auto t0 = std::chrono::steady_clock::now();
+  uint32_t spins = 0;
+  while (h_plan_[kPlanStatusSlot] == 0) {
+    if ((++spins & 1023u) == 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kPlanWaitSeconds) {
+      cuda_check(cudaStreamSynchronize(stream_), "plan sync");
+      break;
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+}
+
 // Plan, size, reserve and apply an append batch whose grouped columns are in
 // key_s_/sa_ (dst)/sb_ (w)/perm_ (original index) and segments in seg_/nseg_.
 // A load sizes the arenas from the plan it reads back. An insert reserves on
@@ -1048,6 +1085,7 @@ unsigned long long* Engine::plan_needs(const StoreView& S, uint64_t k, uint32_t 
 void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t) {
   const uint32_t ks = (uint32_t)std::max<uint64_t>(std::min<uint64_t>(k, n_), 1);
   const StoreView S0 = view();
+  h_plan_[kPlanStatusSlot] = 0;  // k_totals publishes the plan and then a nonzero status here
   plan_needs(S0, k, ks, d_plan_, load_mode ? kReserveNone : kReservePublish);
   auto apply = [&](const StoreView& S, const unsigned long long* dev_base, const HostReserve& hr) {
     launch_pdl(k_apply_insert, grid_for((unsigned long long)ks * 32, kBlock, tuning_.apply_blocks_per_sm), kBlock,
@@ -1058,9 +1096,8 @@ void Engine::run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uin
     ++launches_;
   };
   if (!load_mode) {
-    cuda_check(cudaEventRecord(reserve_ev_, stream_), "reserve");
     apply(S0, base_.as<unsigned long long>(), HostReserve{});
-    cuda_check(cudaEventSynchronize(reserve_ev_), "plan sync");
+    wait_plan();
   } else {
     cuda_check(cudaStreamSynchronize(stream_), "plan sync");
   }

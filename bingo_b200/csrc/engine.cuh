@@ -141,7 +141,6 @@ class Engine {
   volatile unsigned long long* h_plan_ = nullptr;
   unsigned long long* d_plan_ = nullptr;
   cudaEvent_t slots_ev_ = nullptr;  // host-bound slot ids copied out (asynchronous handles)
-  cudaEvent_t reserve_ev_ = nullptr;  // an insert's device reservation is done (its plan is published)
   bool slots_busy_ = false;
   unsigned long long* d_steps_ = nullptr;  // produced walk steps since create
   unsigned long long launches_ = 0;        // hand-written kernels launched since create
@@ -183,6 +182,7 @@ class Engine {
   void group_by_vertex(const uint32_t* key, const uint32_t* a, const uint32_t* b, uint64_t k, bool insert);
   int group_cluster_ok();  // which cluster sizes of the grouping kernel can run here (bit 0: 8, bit 1: 16)
   void run_insert(uint64_t k, uint32_t* dev_out_slots, bool load_mode, uint64_t m_hint);
+  void wait_plan();  // until k_totals has published the insert plan
   unsigned long long* plan_needs(const StoreView& S, uint64_t k, uint32_t ks, volatile unsigned long long* publish,
                                  int reserve);
   void enqueue_insert(const uint32_t* a, const uint32_t* b, const uint32_t* c, uint64_t k, uint32_t* out_slots);
