@@ -542,13 +542,14 @@ unsigned walk_blocks_per_sm() {
 // Default launch shape of each walk kernel (the knobs' value 0), measured on
 // B200 with fixed graphs, launches interleaved: resident 256-thread blocks
 // per SM (0 = the occupancy limit) and walks a warp claims per refill.
-// DeepWalk (config 2's graph): 26.3 G steps/s at 4 blocks and 8 walks
-// against 21.7 G at its 8-block occupancy limit and 32 (more resident warps
-// issue more concurrent random reads than DRAM turns into throughput; 2
-// blocks: 23.0 G). PPR: 11.3 G at 4 blocks and 32 against 11.0 G at 6.
-// node2vec (config 3's graph) and the mixed-app table (config 4's jobs) run
-// best at their occupancy limits (5 and 4 blocks) with 32. One-hop sampling
-// (one step per item) keeps the occupancy limit and 32.
+// DeepWalk (R-MAT scale 20, 16 M edges, log-uniform weights): 26.3 G
+// steps/s at 4 blocks and 8 walks against 21.7 G at its 8-block occupancy
+// limit and 32 (more resident warps issue more concurrent random reads than
+// DRAM turns into throughput; 2 blocks: 23.0 G). PPR: 11.3 G at 4 blocks and
+// 32 against 11.0 G at 6. node2vec (R-MAT scale 22, Zipf weights) and the
+// mixed-app table (R-MAT scale 22, 16 mixed jobs) run best at their
+// occupancy limits (5 and 4 blocks) with 32. One-hop sampling (one step per
+// item) keeps the occupancy limit and 32.
 constexpr unsigned walk_default_bps(int app) { return app == APP_DEEPWALK || app == APP_PPR ? 4 : 0; }
 constexpr uint32_t walk_default_chunk(int app) { return app == APP_DEEPWALK ? 8 : 32; }
 
