@@ -86,33 +86,52 @@ __device__ __forceinline__ int group_of(const GroupIndex& X, unsigned long long 
   return lo;
 }
 
-// Flattened members f0, f0 + stride, ... below end: each names a live slot
-// with the group's bit and the same neighbour, and that slot's back-pointer
-// for the group is the member's position. Returns BINGO_CHECK_MEMBER or 0.
+// The slot whose back-pointer range holds back-pointer index bi: the last
+// slot s < ecnt with ebp(s) <= bi (ebp grows with the slot id), or ecnt if
+// there is none.
+__device__ uint32_t slot_of_bp(const StoreView& S, const VertexMeta& M, uint32_t bi) {
+  uint32_t lo = 0, hi = M.ecnt;  // answer in [lo, hi) or none
+  if (hi == 0 || S.edges[M.eoff].ebp > bi) return M.ecnt;
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (S.edges[M.eoff + mid].ebp <= bi)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Flattened members f0, f0 + stride, ... below end: each holds the
+// back-pointer index of a live slot with the group's bit and the same
+// neighbour (that slot's back-pointer for the group), and that back-pointer
+// is the member's position. Returns BINGO_CHECK_MEMBER or 0.
 __device__ uint32_t check_members(const StoreView& S, const VertexMeta& M, const GroupIndex& X,
                                   unsigned long long f0, unsigned long long stride, unsigned long long end) {
   uint32_t bad = 0;
   for (; f0 < end; f0 += stride * kMemberUnroll) {
     int k[kMemberUnroll];
     unsigned long long pos[kMemberUnroll];
-    uint32_t s[kMemberUnroll], v[kMemberUnroll];
+    uint32_t b[kMemberUnroll], s[kMemberUnroll], v[kMemberUnroll];
     EdgeRec e[kMemberUnroll];
 #pragma unroll
     for (int q = 0; q < kMemberUnroll; ++q) {
       const unsigned long long f = f0 + stride * q;
-      k[q] = 0, pos[q] = 0, s[q] = 0xffffffffu, v[q] = 0;
+      k[q] = 0, pos[q] = 0, b[q] = 0xffffffffu, v[q] = 0;
       if (f < end) {
         k[q] = group_of(X, f);
         pos[q] = f - X.off[k[q]];
         const size_t at = (size_t)X.base[k[q]] * 4 + pos[q];
-        s[q] = S.gs[at];
+        b[q] = S.gs[at];
         v[q] = S.gv[at];
       }
     }
 #pragma unroll
     for (int q = 0; q < kMemberUnroll; ++q) {
       e[q] = EdgeRec{0, 0, 0, 0};
+      s[q] = M.ecnt;
       if (f0 + stride * q >= end) continue;
+      if (b[q] < M.bpcnt) s[q] = slot_of_bp(S, M, b[q]);
       if (s[q] < M.ecnt)
         e[q] = S.edges[M.eoff + s[q]];
       else
@@ -121,12 +140,12 @@ __device__ uint32_t check_members(const StoreView& S, const VertexMeta& M, const
 #pragma unroll
     for (int q = 0; q < kMemberUnroll; ++q) {
       if (f0 + stride * q >= end || s[q] >= M.ecnt) continue;
-      if (!((e[q].w >> k[q]) & 1u) || e[q].v != v[q]) {
+      const unsigned long long bi = (unsigned long long)e[q].ebp + __popc(e[q].w & ((1u << k[q]) - 1u));
+      if (!((e[q].w >> k[q]) & 1u) || e[q].v != v[q] || bi != b[q]) {
         bad = BINGO_CHECK_MEMBER;
         continue;
       }
-      const unsigned long long bi = (unsigned long long)e[q].ebp + __popc(e[q].w & ((1u << k[q]) - 1u));
-      if (bi >= M.bpcnt || S.bp[M.bpoff + bi] != pos[q]) bad = BINGO_CHECK_MEMBER;
+      if (S.bp[M.bpoff + bi] != pos[q]) bad = BINGO_CHECK_MEMBER;
     }
   }
   return bad;

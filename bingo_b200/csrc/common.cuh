@@ -109,7 +109,7 @@ struct StoreView {
   VertexMeta* meta;
   GroupDesc* gdesc;  // [n][32]
   uint32_t* gv;      // member arena: neighbour ids
-  uint32_t* gs;      // member arena: slot ids (same indexing as gv)
+  uint32_t* gs;      // member arena: each member's back-pointer index (its slot's entry for the group; same indexing as gv)
   EdgeRec* edges;
   uint32_t* bp;
   AliasRec* alias;

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "engine.cuh"
 #include "group.cuh"
@@ -2051,25 +2052,30 @@ void Engine::dump(uint32_t* ecnt, uint32_t* live, uint32_t* ev, uint32_t* ew, ui
   HostState H;
   fetch(H, n_, meta_, gdesc_, vrec_, arena_, gs_, h_top_);
   uint64_t s = 0, mem = 0, a = 0;
+  std::vector<uint32_t> ebp;
   for (uint32_t u = 0; u < n_; ++u) {
     const VertexMeta& M = H.meta[u];
     ecnt[u] = M.ecnt;
     live[u] = M.live;
+    ebp.resize(M.ecnt);
     for (uint32_t i = 0; i < M.ecnt; ++i, ++s) {
       const EdgeRec& e = H.edges[M.eoff + i];
       ev[s] = e.v;
       ew[s] = e.w;
+      ebp[i] = e.ebp;
     }
     for (int k = 0; k < kBits; ++k) {
       const GroupDesc& G = H.gd[(size_t)u * kBits + k];
       gcnt[(size_t)u * kBits + k] = G.cnt;
       for (uint32_t p = 0; p < G.cnt; ++p, ++mem) {
+        // A member holds its slot's back-pointer index for the group; the
+        // slot is the last one whose back-pointer range starts at or below it.
         const size_t idx = (size_t)group_base(G) * 4 + p;
-        const uint32_t sl = H.gs[idx];
+        const uint32_t bi = H.gs[idx];
+        const uint32_t sl = (uint32_t)(std::upper_bound(ebp.begin(), ebp.end(), bi) - ebp.begin()) - 1;
         mslot[mem] = sl;
         mv[mem] = H.gv[idx];
-        const EdgeRec& e = H.edges[M.eoff + sl];
-        mbp[mem] = H.bp[M.bpoff + e.ebp + __builtin_popcount(e.w & ((1u << k) - 1u))];
+        mbp[mem] = H.bp[M.bpoff + bi];
       }
     }
     const VertexRec& R = H.vr[u];
@@ -2192,7 +2198,9 @@ struct SnapHeader {
   uint64_t checksum;
 };
 constexpr char kSnapMagic[8] = {'B', 'I', 'N', 'G', 'O', 'S', 'N', 'P'};
-constexpr uint32_t kSnapVersion = 2;  // 2: 8-byte group descriptors, one-member groups named inline in the alias table
+// 2: 8-byte group descriptors, one-member groups named inline in the alias
+// table; 3: members hold back-pointer indices instead of slot ids.
+constexpr uint32_t kSnapVersion = 3;
 constexpr size_t kSnapChunk = 64u << 20;
 
 // Word-wise multiply-xor hash (64-bit lanes, tail bytes folded in one by one).

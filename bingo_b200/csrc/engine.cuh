@@ -129,7 +129,7 @@ class Engine {
   // store
   DevBuf vrec_, meta_, gdesc_;
   DevBuf arena_[kArenas];
-  DevBuf gs_;  // slot ids, parallel to the member arena
+  DevBuf gs_;  // per member, its slot's back-pointer index for the group (parallel to the member arena)
   unsigned long long* d_top_ = nullptr;  // [kArenas]
   unsigned long long cap_[kArenas] = {};
   uint32_t* d_err_ = nullptr;            // [0] ErrBit sticky, [1] rejected deletes

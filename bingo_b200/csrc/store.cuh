@@ -324,11 +324,11 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
       if (out_slots) out_slots[seg_orig[0]] = slot;
     }
     if ((w >> lane) & 1u) {
-      const uint32_t pos = G.cnt;
+      const uint32_t pos = G.cnt, bi = bpbase + __popc(w & ((1u << lane) - 1u));
       const size_t e = (size_t)group_base(G) * 4 + pos;
       S.gv[e] = v;
-      S.gs[e] = slot;
-      S.bp[M.bpoff + bpbase + __popc(w & ((1u << lane) - 1u))] = pos;
+      S.gs[e] = bi;
+      S.bp[M.bpoff + bi] = pos;
       if (pos == 0) single = v;
       ++G.cnt;
     }
@@ -355,11 +355,11 @@ static __device__ void apply_append(const StoreView& S, uint32_t u, const uint32
       const uint32_t b = __ballot_sync(kFull, has);
       const uint32_t kcnt = __shfl_sync(kFull, G.cnt, k), kbase = __shfl_sync(kFull, group_base(G), k);
       if (has) {
-        const uint32_t pos = kcnt + __popc(b & lanemask_lt());
+        const uint32_t pos = kcnt + __popc(b & lanemask_lt()), bi = ebp + __popc(w & ((1u << k) - 1u));
         const size_t e = (size_t)kbase * 4 + pos;
         S.gv[e] = v;
-        S.gs[e] = slot;
-        S.bp[M.bpoff + ebp + __popc(w & ((1u << k) - 1u))] = pos;
+        S.gs[e] = bi;
+        S.bp[M.bpoff + bi] = pos;
       }
       const uint32_t first_v = __shfl_sync(kFull, v, __ffs(b) - 1);  // b != 0: bit k is present
       if (lane == k) {
@@ -468,16 +468,16 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
       const int d = __ffs(r) - 1;
       if ((stage[d] >> lane) & 1u) mine |= 1u << d;
     }
-    // Up to kDeleteRound removals at a time: their members' positions, the
-    // list's last entries and those entries' edge records are loaded
-    // together (two rounds of loads), then the swap-removes run in
-    // registers, in batch order, and are stored. A removal whose member was
-    // moved by an earlier one, or a last entry that an earlier removal
-    // overwrote, is followed in registers (entries are told apart by their
-    // back-pointer index, which is unique per (slot, bit)).
+    // Up to kDeleteRound removals at a time: their members' positions and
+    // the list's last entries (neighbour and back-pointer index) are loaded
+    // together, then the swap-removes run in registers, in batch order, and
+    // are stored. A removal whose member was moved by an earlier one, or a
+    // last entry that an earlier removal overwrote, is followed in registers
+    // (entries are told apart by their back-pointer index, unique per
+    // (slot, bit)). Removing the list's last entry itself moves nothing.
     uint32_t* const bpv = S.bp + M.bpoff;
     while (mine) {
-      uint32_t bpi[kDeleteRound], pos[kDeleteRound], ts[kDeleteRound], tv[kDeleteRound], tbi[kDeleteRound];
+      uint32_t bpi[kDeleteRound], pos[kDeleteRound], tv[kDeleteRound], tbi[kDeleteRound];
       int r = 0;
 #pragma unroll
       for (int q = 0; q < kDeleteRound; ++q) {
@@ -492,18 +492,11 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
       const uint32_t c0 = G.cnt;  // >= r: every removal's member is in the list
 #pragma unroll
       for (int q = 0; q < kDeleteRound; ++q) {
-        pos[q] = ts[q] = tv[q] = tbi[q] = 0;
+        pos[q] = tv[q] = tbi[q] = 0;
         if (q < r) {
           pos[q] = bpv[bpi[q]];
-          ts[q] = S.gs[gb + c0 - 1 - q];
+          tbi[q] = S.gs[gb + c0 - 1 - q];
           tv[q] = S.gv[gb + c0 - 1 - q];
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < kDeleteRound; ++q) {
-        if (q < r) {
-          const EdgeRec em = S.edges[M.eoff + ts[q]];
-          tbi[q] = em.ebp + __popc(em.w & below);
         }
       }
 #pragma unroll
@@ -511,15 +504,17 @@ static __device__ void apply_delete(const StoreView& S, uint32_t u, const uint32
         if (i < r) {
           // Removal i: the entry at the current last position (c0 - 1 - i)
           // moves into the removed member's position p.
-          const uint32_t p = pos[i], ms = ts[i], mv = tv[i], mbi = tbi[i];
-          S.gv[gb + p] = mv;
-          S.gs[gb + p] = ms;
-          bpv[mbi] = p;
-          if (p == 0) front_known = true, front = mv;
+          const uint32_t p = pos[i], mv = tv[i], mbi = tbi[i];
+          if (p != c0 - 1 - i) {
+            S.gv[gb + p] = mv;
+            S.gs[gb + p] = mbi;
+            bpv[mbi] = p;
+            if (p == 0) front_known = true, front = mv;
+          }
 #pragma unroll
           for (int t = i + 1; t < kDeleteRound; ++t) {
-            if (t < r && p == c0 - 1 - t) ts[t] = ms, tv[t] = mv, tbi[t] = mbi;  // a later last entry
-            if (t < r && bpi[t] == mbi) pos[t] = p;                              // a later removal moved
+            if (t < r && p == c0 - 1 - t) tv[t] = mv, tbi[t] = mbi;  // a later last entry
+            if (t < r && bpi[t] == mbi) pos[t] = p;                  // a later removal moved
           }
         }
       }

@@ -73,7 +73,7 @@ def test_check_of_empty_and_edgeless_graphs():
 # File layout: 96-byte header (magic, version, node2vec, n, bits,
 # rec_bytes[4], top[5], payload_bytes, checksum), then VertexRec[n],
 # VertexMeta[n], GroupDesc[n][32], the used part of the member, edge,
-# back-pointer, alias and adjacency arenas, and the member slot ids.
+# back-pointer, alias and adjacency arenas, and the members' back-pointer indices.
 HDR = struct.Struct("<8s4I4I5QQQ")
 MASK = (1 << 64) - 1
 CHUNK = 64 << 20
