@@ -183,10 +183,11 @@ constexpr int kPlanStatusSlot = 2 * kArenas + 1;  // after totals, status word a
 
 // Exclusive prefix of the nb plan-block sums (column-major per arena), in
 // place, and the batch totals per arena (one block; two tiles of
-// kTotalsThreads block sums per barrier pass). With `out` (mapped host memory) it also publishes the insert plan,
-// out[0..5) totals, out[5] the batch status word, out[6..11) the arena tops
-// before this batch, and last (after a system fence) out[kPlanStatusSlot],
-// nonzero once the rest is visible to the host.
+// kTotalsThreads block sums per barrier pass). With `out` (mapped host
+// memory) it also publishes the insert plan: out[0..5) totals, out[5] the
+// batch status word, out[6..11) the arena tops before this batch, and last
+// (after a system fence) out[kPlanStatusSlot], nonzero once the rest is
+// visible to the host.
 // `reserve` != kReserveNone then reserves the batch's arena space, all or
 // nothing: base = the tops, tops += totals. A full arena sets E_CAPACITY in
 // the batch status word (the apply kernel then skips the batch); with
