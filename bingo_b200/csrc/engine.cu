@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "engine.cuh"
@@ -1069,7 +1070,9 @@ void Engine::wait_plan() {
   const auto t0 = std::chrono::steady_clock::now();
   uint32_t spins = 0;
   while (h_plan_[kPlanStatusSlot] == 0) {
-    if ((++spins & 1023u) == 0 &&
+    if (++spins < 4096) continue;  // the plan is usually a few tens of microseconds away
+    std::this_thread::yield();     // a long wait (work queued before the insert) leaves the core to others
+    if ((spins & 255u) == 0 &&
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kPlanWaitSeconds) {
       cuda_check(cudaStreamSynchronize(stream_), "plan sync");
       break;
