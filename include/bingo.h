@@ -311,8 +311,9 @@ int bingo_restore(bingo_handle* h, const char* path);
  *           or a count exceeds its capacity;
  *   COUNT   the live-slot count or a group's member count differs from the
  *           live slots carrying that weight bit;
- *   MEMBER  a group member names a slot that is not live, lacks the group's
- *           bit or holds another neighbour, or its back-pointer disagrees;
+ *   MEMBER  a group member names (through the back-pointer index it holds)
+ *           a slot that is not live, lacks the group's bit or holds another
+ *           neighbour, or its back-pointer disagrees;
  *   ALIAS   the alias table is not the exact table over the group masses
  *           cnt_k * 2^k (slot count, totals, own / alias groups, and for
  *           every group the scaled mass its slots carry);
