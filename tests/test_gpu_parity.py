@@ -1,6 +1,9 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
 same seeded inputs. Graph state (slots, tombstones, group member sequences,
 back-pointers, alias tables) and walks must be bit-exact."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -250,8 +253,8 @@ def test_multi_edges_and_reload():
     assert_exact_equal(g.dump(), ex2.dump())
 
 
-@pytest.mark.parametrize("path", sorted(__import__("glob").glob(
-    __import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "ref_*.npz"))))
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz"))),
+                         ids=os.path.basename)
 def test_cuda_state_matches_reference_binary(path):
     """The CUDA path against the reference's own CUDA build: after the load
     and after every batch, every list the reference keeps (sparse groups in

@@ -143,7 +143,7 @@ def test_golden_fixtures_present():
     assert _golden_cases(), "reference golden fixtures missing (tests/golden/make_golden.py)"
 
 
-@pytest.mark.parametrize("path", _golden_cases())
+@pytest.mark.parametrize("path", _golden_cases(), ids=os.path.basename)
 def test_reference_literal_matches_reference_dumps(path):
     """Pins the CPU restatement to the reference's own CUDA build: the state
     the reference binary dumped after load and after every batch equals the
