@@ -21,6 +21,30 @@ def workload(scale=10, ef=16, seed=11, dist=gen.W_UNIFORM, lo=1, hi=1024, s=1.2,
     return n, src, dst, w, ops
 
 
+def chisq_pvalue(counts, probs):
+    """Pearson chi-square p-value of sampled counts against exact
+    probabilities; bins whose expected count is below 5 are pooled into one
+    (the chi-square approximation needs expected counts >= 5, and log-uniform
+    weights give neighbours of probability ~1e-8). A draw of a
+    zero-probability bin fails outright."""
+    from scipy import stats
+    counts = np.asarray(counts, np.float64)
+    exp = np.asarray(probs, np.float64) * counts.sum()
+    zero = exp == 0
+    assert counts[zero].sum() == 0, "sampled a zero-probability neighbour"
+    big = exp >= 5
+    small = ~big & ~zero
+    obs_b, exp_b = list(counts[big]), list(exp[big])
+    if small.any():
+        obs_b.append(counts[small].sum())
+        exp_b.append(exp[small].sum())
+        if exp_b[-1] < 5 and len(exp_b) > 1:  # fold a still-small pool into the smallest bin
+            j = int(np.argmin(exp_b[:-1]))
+            obs_b[j] += obs_b.pop()
+            exp_b[j] += exp_b.pop()
+    return stats.chisquare(np.array(obs_b), np.array(exp_b)).pvalue
+
+
 def csr_offsets(counts):
     off = np.zeros(len(counts) + 1, np.int64)
     np.cumsum(counts, out=off[1:])

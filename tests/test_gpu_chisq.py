@@ -4,32 +4,12 @@ P(v | u) = sum of w(u, v) / sum of w(u, .), by Pearson's chi-square test at
 significance alpha = 1e-3 per vertex (Bonferroni over the vertices tested)."""
 import numpy as np
 import pytest
-from scipy import stats
 
 from bingo_b200 import DEEPWALK, SAMPLING, Graph, gen
+from tests.helpers import chisq_pvalue as _chisq
 
 pytestmark = pytest.mark.gpu
 ALPHA = 1e-3
-
-
-def _chisq(counts, probs):
-    """Pearson chi-square p-value; neighbours whose expected count is below 5
-    are pooled into one bin (the chi-square approximation needs expected
-    counts >= 5, and log-uniform weights give neighbours of probability ~1e-8)."""
-    exp = probs * counts.sum()
-    zero = exp == 0
-    assert counts[zero].sum() == 0, "sampled a zero-probability neighbour"
-    big = exp >= 5
-    small = ~big & ~zero
-    obs_b, exp_b = list(counts[big]), list(exp[big])
-    if small.any():
-        obs_b.append(counts[small].sum())
-        exp_b.append(exp[small].sum())
-        if exp_b[-1] < 5 and len(exp_b) > 1:  # fold a still-small pool into the smallest bin
-            j = int(np.argmin(exp_b[:-1]))
-            obs_b[j] += obs_b.pop()
-            exp_b[j] += exp_b.pop()
-    return stats.chisquare(np.array(obs_b), np.array(exp_b)).pvalue
 
 
 def test_one_hop_distribution_handmade():
