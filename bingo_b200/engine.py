@@ -128,6 +128,8 @@ class Graph:
             raise BingoError(st, (self._L.bingo_last_error(self._h) or b"").decode())
 
     def close(self):
+        """Destroy the handle (bingo_destroy): frees the graph arenas, staging
+        buffers and streams. Idempotent."""
         if getattr(self, "_h", None):
             self._L.bingo_destroy(self._h)
             self._h = None
@@ -315,6 +317,8 @@ class Graph:
                 "latency_ns": s.latency_ns, "ready_ns": s.ready_ns}
 
     def serve_poll(self, ticket: int) -> dict:
+        """Status of a serving ticket without waiting: done flag, request status,
+        kind, graph version, latency and ready time."""
         s = BingoServeStatus()
         self._check(self._L.bingo_serve_poll(self._h, ticket, ctypes.byref(s)))
         return self._status(s)
@@ -430,21 +434,30 @@ class Graph:
         return out
 
     def serve_metrics(self) -> dict:
+        """Serving counters: submitted and completed requests, walk-kernel launches,
+        scheduler time per phase (admission, completion, updates, drain waits) and
+        the summed queue, device and copy time of walk queries."""
         m = BingoServeMetrics()
         self._check(self._L.bingo_serve_get_metrics(self._h, ctypes.byref(m)))
         return {f: getattr(m, f) for f, _ in BingoServeMetrics._fields_}
 
     def serve_stop(self):
+        """Finish every submitted request, stop the walk loop and return the handle to normal use."""
         self._check(self._L.bingo_serve_stop(self._h))
         self._serve_keep = {}
 
     def sync(self):
+        """Wait for all queued work; raises the first device-detected error since the last sync."""
         self._check(self._L.bingo_sync(self._h))
 
     def set_stream(self, stream_ptr: int):
+        """Order later calls on a caller's CUDA stream (its handle as an int, e.g.
+        torch.cuda.Stream().cuda_stream); 0 restores the handle's own stream."""
         self._check(self._L.bingo_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
     def stats(self) -> dict:
+        """Counts (vertices, slots, live edges), arena and scratch bytes, walk steps,
+        kernel launches and node2vec proposals / adjacency probes since creation."""
         s = BingoStats()
         self._check(self._L.bingo_get_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in BingoStats._fields_ if f != "reserved0"}
@@ -467,6 +480,8 @@ class Graph:
         return d
 
     def philox(self, ctr: np.ndarray, key: int) -> np.ndarray:
+        """Philox4x32-10 blocks as the walk kernels compute them: one row of four
+        words out per row of four counter words in, under the 64-bit key."""
         ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
         out = np.zeros_like(ctr)
         self._check(self._L.bingo_philox(self._h, ctypes.c_void_p(ctr.ctypes.data), ctr.shape[0], key,
