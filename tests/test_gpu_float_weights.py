@@ -9,8 +9,8 @@ import pytest
 
 from bingo_b200 import DEEPWALK, NODE2VEC, PPR, SAMPLING, BingoError, Graph, fixed16, gen
 from oracle import pyoracle as po
-from tests.helpers import assert_exact_equal
-from tests.test_gpu_chisq import ALPHA, _chisq
+from tests.helpers import assert_exact_equal, chisq_pvalue as _chisq
+from tests.test_gpu_chisq import ALPHA
 
 pytestmark = pytest.mark.gpu
 

@@ -3,7 +3,9 @@ one-hop draws against P(v | u) = w(u, v) / sum of w(u, .)
 (include/Bingo.cuh:220-267), node2vec second steps against
 w(cur, x) * alpha(prev, x) (include/operation.cuh:281-335, with the
 neighbour test on N(prev)), and PPR walk lengths against the geometric stop
-of include/operation.cuh:336-368. Pearson's chi-square at alpha = 1e-3 per
+of include/operation.cuh:336-368, and one-hop draws of 16.16 fixed-point
+weights against the float weights they quantise (include/Bingo.cuh:65-69,
+:254-264). Pearson's chi-square at alpha = 1e-3 per
 test (Bonferroni over the vertices where several are tested). The CUDA walks
 equal the oracle's bit for bit, so this pins both to the distributions."""
 import numpy as np
@@ -108,3 +110,19 @@ def test_ppr_stops_geometrically(stop):
     probs[-1] = (1 - stop) ** (L - 2)
     pv = chisq_pvalue(np.bincount(moves, minlength=L)[1:], probs)
     assert pv > ALPHA, (stop, pv)
+
+
+def test_float_weights_one_hop():
+    """Float-weight mode's parity definition on the oracle: weights quantised
+    to 16.16 fixed point (bingo_weights_to_fixed16) and loaded as integers
+    give one-hop draws that pass against the float weights themselves (the
+    quantisation moves each probability by at most 2^-17 / w relative)."""
+    from bingo_b200 import fixed16
+    n = 64
+    w = np.array([0.001, 0.37, 1.0, 2.5, 3.25, 17.125, 999.9, 12345.678, 65535.5, 0.75], np.float32)
+    ex = po.ExactGraph(n)
+    ex.load(np.zeros(len(w), np.uint32), np.arange(1, len(w) + 1, dtype=np.uint32), fixed16(w))
+    out = ex.walk(SAMPLING, 1, np.zeros(1_000_000, np.uint32), seed=77)
+    probs = w.astype(np.float64) / w.astype(np.float64).sum()
+    pv = chisq_pvalue(np.bincount(out, minlength=n)[1:len(w) + 1], probs)
+    assert pv > ALPHA, pv
