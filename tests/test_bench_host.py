@@ -1,6 +1,7 @@
 """Host logic of bench.py that needs no GPU: the default line's summary of
-the node2vec / batched / served / reference-CUDA child runs, and the
-profiler guard that keeps child runs out of an ncu capture."""
+the node2vec / batched / served / reference-CUDA child runs, the profiler
+guard that keeps child runs out of an ncu capture, and the reference arm's
+other ranks under torchrun."""
 import bench
 
 
@@ -54,3 +55,16 @@ def test_profiler_guard(monkeypatch):
     assert not bench.under_profiler()
     monkeypatch.setenv("CUDA_INJECTION64_PATH", "/x/libinjection.so")
     assert bench.under_profiler()
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun with N > 1 the reference arm runs on rank 0 alone; every
+    other rank exits 0 at once, prints nothing and joins no collective."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1", MASTER_ADDR="127.0.0.1", MASTER_PORT="1")
+    r = subprocess.run([sys.executable, bench.__file__, "--impl", "reference", "--gpus", "2", "--steps", "2",
+                        "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-800:]
+    assert r.stdout.strip() == ""
